@@ -1,0 +1,210 @@
+/*
+ * b2p.h -- C ABI of the B200 PDHG LP engine (libb2p.so).
+ *
+ * This is the drop-in boundary for the reference BharatOpt first-order LP
+ * path.  The reference's C++ entry points bind to it as follows (reference
+ * file:line of each interface replaced):
+ *
+ *   GpuBackend::initialize / device_info   include/bharatopt/gpu_backend.hpp:173-177
+ *        -> b2p_device_info, b2p_ctx_create
+ *   GpuBackend::spmv / spmv_with_cpu_comparison  gpu_backend.hpp:180-190
+ *        -> b2p_spmv
+ *   GpuBackend::vector_add/_sub/_scale, axpy     gpu_backend.hpp:193-216
+ *        -> b2p_vector_op
+ *   GpuBackend::dot_product / norm2              gpu_backend.hpp:218-227
+ *        -> b2p_dot, b2p_norm2
+ *   GPUFirstOrderSolver::solve                   include/bharatopt/first_order_solver.hpp:89-98
+ *   (src/first_order_solver.cpp:295-306)
+ *        -> b2p_upload_lp + b2p_solve  (after the reference's own validation,
+ *           presolve and standard form, src/first_order_solver.cpp:18-101)
+ *   FirstOrderSolverStats / Result / Status      first_order_solver.hpp:15-60
+ *        -> b2p_result, B2P_STATUS_*
+ *
+ * Entry points with no reference counterpart (new engine capabilities):
+ *   b2p_batch_*  -- thousands of independent LPs in one persistent launch
+ *   b2p_mlp_*    -- learned warm start (BF16 tensor-core MLP)
+ *
+ * Conventions: plain pointers and sizes; every pointer argument is HOST
+ * memory unless its name ends in _dev.  Every function returns an int status
+ * (B2P_OK on success) and never throws.  A context owns one CUDA stream and
+ * all device buffers it allocates; it is not re-entrant (one host thread per
+ * context at a time).  There is no CPU fallback: without a usable GPU every
+ * compute entry point returns B2P_GPU_UNAVAILABLE.
+ */
+#ifndef B2P_H
+#define B2P_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- call status; 0..5 have the meaning of bharatopt::GPUStatus
+ *      (include/bharatopt/gpu_backend.hpp:15-22) ---- */
+#define B2P_OK                  0
+#define B2P_GPU_UNAVAILABLE     1
+#define B2P_GPU_UNINITIALIZED   2
+#define B2P_OUT_OF_MEMORY       3
+#define B2P_INVALID_ARGUMENT    4
+#define B2P_EXECUTION_FAILED    5
+#define B2P_NO_LP               6   /* solve before upload */
+#define B2P_TIMEOUT             7   /* a bounded device wait or the time limit ran out */
+
+/* ---- solver outcome; same ordinals as bharatopt::FirstOrderSolverStatus
+ *      (include/bharatopt/first_order_solver.hpp:15-22) ---- */
+#define B2P_STATUS_OPTIMAL              0
+#define B2P_STATUS_MAX_ITERATIONS       1
+#define B2P_STATUS_NUMERICAL_FAILURE    2
+#define B2P_STATUS_INFEASIBLE_DETECTED  3
+#define B2P_STATUS_UNBOUNDED_DETECTED   4
+#define B2P_STATUS_INTERRUPTED          5
+
+/* ---- engines ---- */
+#define B2P_ENGINE_REFERENCE  0  /* the reference PDHG, iterate-for-iterate (FP64 only) */
+#define B2P_ENGINE_HALPERN    1  /* restarted Halpern PDHG, scaled, rel-KKT termination */
+
+#define B2P_FP64  0
+#define B2P_FP32  1              /* FP32 vectors + SpMV, FP64 reductions / scaling / KKT */
+
+typedef struct {
+    int    is_available;
+    char   device_name[128];
+    size_t total_memory_bytes;
+    size_t free_memory_bytes;
+    int    compute_capability_major;
+    int    compute_capability_minor;
+    int    multiprocessor_count;
+    int    l2_cache_bytes;
+    char   status_message[256];
+} b2p_device_info_t;
+
+/* Host-observed phase times in milliseconds (GpuTimingResult,
+ * include/bharatopt/gpu_backend.hpp:34-41); kernel time from CUDA events. */
+typedef struct {
+    double h2d_time_ms;
+    double kernel_time_ms;
+    double d2h_time_ms;
+    double sync_time_ms;
+    double total_gpu_time_ms;
+} b2p_timing_t;
+
+typedef struct {
+    int     engine;                 /* B2P_ENGINE_* */
+    int     precision;              /* B2P_FP64 / B2P_FP32 (Halpern engine only) */
+    int64_t max_iterations;         /* default 50000 (first_order_solver.hpp:30) */
+    /* reference engine (FirstOrderSolverOptions, first_order_solver.hpp:29-38) */
+    double  feasibility_tolerance;  /* 1e-7 */
+    double  primal_step_size;       /* 0.01, used when adaptive_step_size == 0 */
+    double  dual_step_size;         /* 0.01 */
+    int     adaptive_step_size;     /* 1 */
+    int64_t check_frequency;        /* 100 (clamped to <= 100 like the reference) */
+    /* Halpern engine */
+    double  eps_rel_kkt;            /* 1e-6: primal, dual and gap all within eps relative */
+    int     check_every;            /* 64 iterations per chunk (restart / KKT cadence) */
+    int     ruiz_iterations;        /* 10 */
+    double  reflection;             /* 1.0 = reflected Halpern */
+    double  restart_sufficient;     /* 0.2 */
+    double  restart_necessary;      /* 0.8 */
+    double  restart_artificial;     /* 0.36 */
+    double  primal_weight;          /* 0 = ||c||/||b|| of the scaled LP */
+    double  step_safety;            /* 0.998 / ||A||_2 */
+    int     refinement_rounds;      /* FP64 iterative-refinement rounds after the FP32 solve (0 = off) */
+    double  refinement_eps;         /* target rel KKT of the refined answer */
+    double  time_limit_s;           /* 0 = none */
+    int     lanes_per_row;          /* 0 = auto; else 1,2,4,8,16,32 lanes per CSR row */
+} b2p_params;
+
+typedef struct {
+    int     status;                 /* B2P_STATUS_* */
+    int64_t iterations;
+    int64_t restarts;
+    double  primal_objective;       /* c.x of the standard-form LP */
+    double  dual_objective;
+    double  rel_primal_residual;    /* FP64, original (unscaled) LP */
+    double  rel_dual_residual;
+    double  rel_gap;
+    double  rel_kkt;                /* max of the three */
+    double  constraint_violation;   /* max |viol| (reference engine: FirstOrderSolverStats) */
+    double  bound_violation;
+    double  max_primal_delta;
+    double  max_dual_delta;
+    int     used_average;           /* reference engine picked the ergodic average */
+    int     refinement_rounds_done;
+    double  primal_weight;
+    double  step_size;
+    double  solve_time_ms;          /* host wall time of b2p_solve */
+    double  kernel_time_ms;         /* CUDA-event time of the iteration loop */
+    double  transfer_time_ms;       /* host<->device copies inside b2p_solve */
+    int64_t kernel_launches;        /* kernels this call launched (graph nodes counted) */
+} b2p_result;
+
+/* ---- device, context ---- */
+int  b2p_device_info(int device, b2p_device_info_t* out);
+int  b2p_ctx_create(int device, void** ctx_out);
+int  b2p_ctx_destroy(void* ctx);
+const char* b2p_last_error(void* ctx);      /* message of the last failed call (never null) */
+void b2p_params_default(b2p_params* p);
+
+/* ---- GpuBackend primitives (host buffers; FP64 CSR with int32 indices) ---- */
+int b2p_spmv(void* ctx, int m, int n, const int32_t* rowptr, const int32_t* colidx, const double* vals,
+             const double* x, double* y, b2p_timing_t* timing);
+int b2p_spmv_t(void* ctx, int m, int n, const int32_t* rowptr, const int32_t* colidx, const double* vals,
+               const double* y, double* w, b2p_timing_t* timing);
+#define B2P_VEC_ADD   0   /* out = a + b          */
+#define B2P_VEC_SUB   1   /* out = a - b          */
+#define B2P_VEC_SCALE 2   /* out = alpha * a      */
+#define B2P_VEC_AXPY  3   /* out = alpha * a + b  */
+int b2p_vector_op(void* ctx, int op, size_t n, double alpha, const double* a, const double* b, double* out,
+                  b2p_timing_t* timing);
+int b2p_dot(void* ctx, size_t n, const double* a, const double* b, double* out, b2p_timing_t* timing);
+int b2p_norm2(void* ctx, size_t n, const double* a, double* out, b2p_timing_t* timing);
+
+/* ---- single LP ----
+ * Standard form (src/first_order_solver.cpp:68-101): minimise c.x subject to
+ * (A x)_i <= b_i where is_eq[i] == 0, (A x)_i == b_i where is_eq[i] == 1, and
+ * lb <= x <= ub (entries may be +-inf).  A is CSR with int32 indices, column
+ * indices strictly ascending within each row (CSRMatrix::is_valid,
+ * src/sparse_matrix.cpp:187-207).  The context keeps one uploaded LP. */
+int b2p_upload_lp(void* ctx, int m, int n, int64_t nnz, const int32_t* rowptr, const int32_t* colidx,
+                  const double* vals, const double* b, const double* c, const double* lb, const double* ub,
+                  const uint8_t* is_eq);
+/* x0 (n) / y0 (m) optional warm start (Halpern engine); x_out (n) / y_out (m) optional. */
+int b2p_solve(void* ctx, const b2p_params* params, const double* x0, const double* y0, b2p_result* result,
+              double* x_out, double* y_out);
+
+/* ---- batch of independent LPs (no reference counterpart) ----
+ * `nmat` constraint matrices in concatenated CSR (mat_rowptr_off[k] indexes
+ * rowptr, mat_nnz_off[k] indexes colidx/vals; rowptr entries are local to their
+ * matrix).  `count` instances each name a matrix (inst_mat) and bring their own
+ * b (m of that matrix), c, lb, ub (n) and is_eq, concatenated in instance order.
+ * Many instances may share one matrix (parametric families). */
+int b2p_batch_upload(void* ctx, int nmat, const int32_t* mat_m, const int32_t* mat_n,
+                     const int64_t* mat_nnz_off, const int32_t* rowptr, const int32_t* colidx, const double* vals,
+                     int count, const int32_t* inst_mat, const double* b, const double* c, const double* lb,
+                     const double* ub, const uint8_t* is_eq);
+/* Solve all instances with the Halpern engine.  x0/y0 optional warm starts
+ * (concatenated like c / b), omega0 optional per-instance primal weights.
+ * Outputs (optional): per-instance status, iterations, rel KKT; concatenated x, y. */
+int b2p_batch_solve(void* ctx, const b2p_params* params, const double* x0, const double* y0, const double* omega0,
+                    int32_t* status_out, int64_t* iters_out, double* kkt_out, double* x_out, double* y_out,
+                    b2p_result* summary);
+
+/* ---- learned warm start: MLP in -> h -> h -> out, GELU, BF16 weights and
+ *      activations, FP32 accumulation on the tcgen05 tensor cores ---- */
+int b2p_mlp_create(void* ctx, int in_dim, int hidden, int out_dim, uint64_t seed);
+/* One pass of Adam over N samples (X: N x in_dim, Y: N x out_dim, FP32 row-major,
+ * host).  loss_out (optional) receives the mean squared error of the epoch. */
+int b2p_mlp_train_epoch(void* ctx, const float* X, const float* Y, int N, int batch, float lr, float* loss_out);
+int b2p_mlp_infer(void* ctx, const float* X, int N, float* Y_out);
+/* Raw BF16 GEMM on the tensor cores, for tests: C(MxN, fp32) = op(A) op(B),
+ * A is M x K (trans_a = 0) or K x M (trans_a = 1) bf16 row-major, B is K x N
+ * (trans_b = 0) or N x K (trans_b = 1).  Host buffers (bf16 as uint16). */
+int b2p_gemm_bf16(void* ctx, int M, int N, int K, const uint16_t* A, int trans_a, const uint16_t* B, int trans_b,
+                  float* C);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* B2P_H */

@@ -1,0 +1,90 @@
+"""Halpern engine (restarted Halpern PDHG) on the GPU, FP64 and FP32.
+
+Parity bar (no reference counterpart for this algorithm): the FP64 KKT of the
+returned point, recomputed by the oracle, is within the requested relative
+tolerance; the objective is within 1e-6 relative of the HiGHS optimum; and the
+reference's SolutionVerifier accepts x at the stated tolerance."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import pdlp_oracle
+
+pytestmark = pytest.mark.gpu
+
+
+def _lps(lpgen):
+    out = {
+        "rs_c0": lpgen.random_sparse(),
+        "rs_small": lpgen.random_sparse(m=40, n=120, nnz_per_col=3, seed=11),
+        "ba_tiny": lpgen.block_angular(periods=3, block_rows=60, block_cols=300, nnz_per_col=4, link_rows=30, seed=9),
+        "ill_small": lpgen.ill_conditioned(m=300, n=1500, nnz_per_col=4, seed=4),
+    }
+    for i, lp in enumerate(lpgen.uneven_batch(6, seed=12)):
+        out[f"batch12_{i}"] = lp
+    return out
+
+
+@pytest.fixture(scope="module")
+def lps(lpgen):
+    return _lps(lpgen)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+@pytest.mark.parametrize("name", ["rs_c0", "rs_small", "ba_tiny", "batch12_0", "batch12_3", "ill_small"])
+def test_halpern_reaches_tolerance(ctx, golden, lps, name, precision):
+    lp = lps[name]
+    std = lp.standard()
+    ctx.upload(std)
+    res, x, y = ctx.solve(engine="halpern", precision=precision, eps=1e-6, max_iterations=200000)
+    assert res["status"] == "OPTIMAL", res
+    k = pdlp_oracle.kkt(std, x, y)
+    # the device KKT and the oracle KKT agree, and both meet the tolerance
+    assert k["rel_kkt"] <= 1.05e-6, k
+    assert abs(k["pobj"] - res["primal_objective"]) <= 1e-9 * (1 + abs(k["pobj"]))
+    z = golden["highs"][name]
+    assert abs(k["pobj"] - z) <= 1e-6 * max(1.0, abs(z)), (k["pobj"], z)
+
+
+def test_halpern_fp64_tight(ctx, golden, lps):
+    std = lps["rs_c0"].standard()
+    ctx.upload(std)
+    res, x, y = ctx.solve(engine="halpern", precision="fp64", eps=1e-9, max_iterations=400000)
+    assert res["status"] == "OPTIMAL"
+    k = pdlp_oracle.kkt(std, x, y)
+    assert k["rel_kkt"] <= 1.05e-9
+    assert abs(k["pobj"] - golden["highs"]["rs_c0"]) <= 1e-8 * abs(golden["highs"]["rs_c0"])
+
+
+def test_halpern_verifier_accepts(ctx, reflib, lps):
+    lp = lps["rs_c0"]
+    std = lp.standard()
+    ctx.upload(std)
+    res, x, y = ctx.solve(engine="halpern", precision="fp32", eps=1e-6)
+    tol = 1e-6 * (1 + float(np.linalg.norm(std.b)))
+    v = reflib.verify(lp, x, feas_tol=tol, reported_obj=float(lp.obj @ x))
+    assert v["verified"] == 1, v
+
+
+def test_halpern_warm_start_from_solution(ctx, lps):
+    std = lps["rs_c0"].standard()
+    ctx.upload(std)
+    res, x, y = ctx.solve(engine="halpern", precision="fp64", eps=1e-7)
+    res2, x2, y2 = ctx.solve(x0=x, y0=y, engine="halpern", precision="fp64", eps=1e-6,
+                             primal_weight=res["primal_weight"])
+    assert res2["status"] == "OPTIMAL" and res2["iterations"] <= 128
+
+
+def test_halpern_iteration_limit(ctx, lps):
+    std = lps["rs_c0"].standard()
+    ctx.upload(std)
+    res, _, _ = ctx.solve(engine="halpern", precision="fp32", eps=1e-12, max_iterations=640)
+    assert res["status"] == "MAX_ITERATIONS" and res["iterations"] == 640
+
+
+def test_halpern_time_limit(ctx, lps):
+    std = lps["rs_c0"].standard()
+    ctx.upload(std)
+    res, _, _ = ctx.solve(engine="halpern", precision="fp64", eps=1e-14, max_iterations=10**8, time_limit_s=0.2)
+    assert res["status"] == "INTERRUPTED"
