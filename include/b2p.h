@@ -145,6 +145,10 @@ int  b2p_device_info(int device, b2p_device_info_t* out);
 int  b2p_ctx_create(int device, void** ctx_out);
 int  b2p_ctx_destroy(void* ctx);
 const char* b2p_last_error(void* ctx);      /* message of the last failed call (never null) */
+/* Run all of this context's work on the caller's CUDA stream (cudaStream_t passed
+ * as void*; null restores the context's own stream).  Lets a caller order and
+ * time the engine's kernels with its own events. */
+int  b2p_ctx_set_stream(void* ctx, void* stream);
 void b2p_params_default(b2p_params* p);
 
 /* ---- GpuBackend primitives (host buffers; FP64 CSR with int32 indices) ---- */
@@ -173,6 +177,15 @@ int b2p_upload_lp(void* ctx, int m, int n, int64_t nnz, const int32_t* rowptr, c
 /* x0 (n) / y0 (m) optional warm start (Halpern engine); x_out (n) / y_out (m) optional. */
 int b2p_solve(void* ctx, const b2p_params* params, const double* x0, const double* y0, b2p_result* result,
               double* x_out, double* y_out);
+
+/* Per-kernel timing of the Halpern iteration on the uploaded LP, after a
+ * b2p_solve with the same params: `reps` plain iterations launched one kernel
+ * at a time between CUDA events on the context stream.  Returns the mean
+ * duration of the primal kernel (A^T y + primal step) and of the dual kernel
+ * (A xh + dual step) and the algorithmic bytes each moves per launch (every
+ * matrix entry, row pointer and vector element read or written once). */
+int b2p_kernel_timing(void* ctx, const b2p_params* params, int reps, double* primal_ms, double* dual_ms,
+                      double* primal_bytes, double* dual_bytes);
 
 /* ---- batch of independent LPs (no reference counterpart) ----
  * `nmat` constraint matrices in concatenated CSR (mat_rowptr_off[k] indexes

@@ -76,6 +76,9 @@ SIGNATURES = {
     "b2p_ctx_destroy": (C.c_int, [_P]),
     "b2p_last_error": (C.c_char_p, [_P]),
     "b2p_params_default": (None, [C.POINTER(Params)]),
+    "b2p_ctx_set_stream": (C.c_int, [_P, _P]),
+    "b2p_kernel_timing": (C.c_int, [_P, C.POINTER(Params), C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double),
+                                    C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "b2p_spmv": (C.c_int, [_P, C.c_int, C.c_int, _I32P, _I32P, _F64P, _F64P, _F64P, C.POINTER(Timing)]),
     "b2p_spmv_t": (C.c_int, [_P, C.c_int, C.c_int, _I32P, _I32P, _F64P, _F64P, _F64P, C.POINTER(Timing)]),
     "b2p_vector_op": (C.c_int, [_P, C.c_int, C.c_size_t, C.c_double, _F64P, _P, _F64P, C.POINTER(Timing)]),
@@ -182,6 +185,18 @@ class Context:
     def _check(self, st):
         if st != OK:
             raise B2PError(st, lib().b2p_last_error(self._h).decode())
+
+    def set_stream(self, stream_handle):
+        """Issue all work on an existing cudaStream_t (an int handle, e.g. torch's
+        `torch.cuda.current_stream().cuda_stream`); None restores the context's own."""
+        self._check(lib().b2p_ctx_set_stream(self._h, C.c_void_p(stream_handle) if stream_handle else None))
+
+    def kernel_timing(self, reps=20, **params):
+        p = default_params(**params)
+        vals = [C.c_double() for _ in range(4)]
+        self._check(lib().b2p_kernel_timing(self._h, C.byref(p), reps, *[C.byref(v) for v in vals]))
+        return {"primal_ms": vals[0].value, "dual_ms": vals[1].value, "primal_bytes": vals[2].value,
+                "dual_bytes": vals[3].value}
 
     # ---- GpuBackend primitives
     def spmv(self, m, n, rowptr, colidx, vals, x, transpose=False):

@@ -280,13 +280,36 @@ int b2p_ctx_create(int device, void** ctx_out) {
     ctx->device = device;
     ctx->sm_count = info.multiprocessor_count;
     ctx->l2_bytes = info.l2_cache_bytes;
-    if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess ||
+    if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreate(&ctx->ev0) != cudaSuccess || cudaEventCreate(&ctx->ev1) != cudaSuccess) {
         delete ctx;
         return B2P_GPU_UNAVAILABLE;
     }
+    ctx->stream = ctx->own_stream;
     *ctx_out = ctx;
     return B2P_OK;
+}
+
+int b2p_ctx_set_stream(void* p, void* stream) {
+    Ctx* ctx = as_ctx(p);
+    if (!ctx) return B2P_GPU_UNINITIALIZED;
+    cudaSetDevice(ctx->device);
+    B2P_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    ctx->stream = stream ? static_cast<cudaStream_t>(stream) : ctx->own_stream;
+    return B2P_OK;
+}
+
+int b2p_kernel_timing(void* p, const b2p_params* params, int reps, double* primal_ms, double* dual_ms,
+                      double* primal_bytes, double* dual_bytes) {
+    Ctx* ctx = as_ctx(p);
+    if (!ctx) return B2P_GPU_UNINITIALIZED;
+    if (!ctx->has_lp || !ctx->hw) {
+        ctx->err = "b2p_kernel_timing: solve an uploaded LP with the Halpern engine first";
+        return B2P_NO_LP;
+    }
+    if (!params || reps <= 0) return B2P_INVALID_ARGUMENT;
+    cudaSetDevice(ctx->device);
+    return halpern_kernel_timing(ctx, params, reps, primal_ms, dual_ms, primal_bytes, dual_bytes);
 }
 
 int b2p_ctx_destroy(void* p) {
@@ -301,7 +324,7 @@ int b2p_ctx_destroy(void* p) {
     new (&ctx->lp) DevLP();
     if (ctx->ev0) cudaEventDestroy(ctx->ev0);
     if (ctx->ev1) cudaEventDestroy(ctx->ev1);
-    if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
     delete ctx;
     return B2P_OK;
 }

@@ -89,7 +89,8 @@ struct Ctx {
     int device = 0;
     int sm_count = 148;
     int l2_bytes = 0;
-    cudaStream_t stream = nullptr;
+    cudaStream_t stream = nullptr;       // stream all work is issued on
+    cudaStream_t own_stream = nullptr;   // the context's own stream
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     std::string err;
     bool has_lp = false;
@@ -126,6 +127,8 @@ int build_transpose(Ctx* ctx, int m, int n, int64_t nnz, const int32_t* rowptr, 
 int ref_engine_solve(Ctx* ctx, const b2p_params* p, b2p_result* r, double* x_out, double* y_out);
 int halpern_engine_solve(Ctx* ctx, const b2p_params* p, const double* x0, const double* y0, b2p_result* r,
                          double* x_out, double* y_out);
+int halpern_kernel_timing(Ctx* ctx, const b2p_params* p, int reps, double* primal_ms, double* dual_ms,
+                          double* primal_bytes, double* dual_bytes);
 void halpern_free(Ctx* ctx);
 void batch_free(Ctx* ctx);
 void mlp_free(Ctx* ctx);

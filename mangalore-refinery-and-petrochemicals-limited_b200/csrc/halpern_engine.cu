@@ -1,5 +1,13 @@
-// Halpern engine: restarted Halpern PDHG with reflection on a diagonally scaled
-// LP, FP32 or FP64 iterates, FP64 reductions, scaling and KKT.
+// Halpern engine: restarted Halpern PDHG with reflection on a diagonally scaled LP.
+//
+// Precision: B2P_FP64 keeps everything in FP64.  B2P_FP32 (mixed) stores the
+// scaled matrix values (the bytes that dominate an iteration) and the gathered
+// operand xh of A xh in FP32, while the Halpern iterates x, y, their anchors,
+// the y gathered by A^T y, every accumulation, the scaling, the restart
+// residuals and the KKT stay FP64.  Measured on the random-sparse family:
+// FP32 iterates cost 1.8-3x more iterations and an FP32 copy of y for the A^T y
+// gather stalls convergence (the reduced costs c + A^T y cancel); FP32 values
+// and an FP32 xh cost none.
 //
 // Problem (standard form of src/first_order_solver.cpp:68-101):
 //   min c.x  s.t. (Ax)_i <= b_i (<= rows) / = b_i (= rows),  l <= x <= u,
@@ -54,10 +62,14 @@ struct HalpernWork {
     DBuf<double> sv64, stv64;      // scaled A and A^T, FP64 (KKT, power iteration, FP64 engine)
     DBuf<float> sv32, stv32;       // scaled A and A^T, FP32 (FP32 engine)
     DBuf<double> c64, b64, l64, u64;
-    DBuf<float> c32, b32, l32, u32;
-    DBuf<double> x64, xh64, xa64, xt64, y64, ya64, yt64;
-    DBuf<float> x32, xh32, xa32, xt32, y32, ya32, yt32;
+    DBuf<double> x, xa, xt, y, ya, yt;  // FP64 iterates (both precisions)
+    DBuf<double> xh64;                   // gathered operand, FP64 engine
+    DBuf<float> xh32, yg32;              // gathered operands, mixed engine
     DBuf<Ctrl> ctrl;
+    // autotuned launch shape (lanes per row L, rows per lane group R) of the two
+    // iteration kernels, keyed by the LP's shape and precision
+    long long tuned_key = -1;
+    int Lc = 8, Rc = 1, Lr = 8, Rr = 1;
     Ctrl* host_ctrl = nullptr;     // pinned, 2 slots
     cudaEvent_t ev[2] = {nullptr, nullptr};
     ~HalpernWork() {
@@ -195,99 +207,156 @@ __global__ void k_pow_init(int n, double* __restrict__ v) {
 }
 
 // ------------------------------------------------------------------ iterate init
-template <typename T>
-__global__ void k_init_iterates(int m, int n, const T* __restrict__ l, const T* __restrict__ u,
-                                const double* __restrict__ x0s, const double* __restrict__ y0s,
-                                const uint8_t* __restrict__ is_eq, T* x, T* xa, T* xt, T* y, T* ya, T* yt) {
+// x, xa, xt <- clamp(x0 / dc) ; y, ya, yt <- P_Y(y0 / dr) (warm start given in original space)
+__global__ void k_init_iterates(int m, int n, const double* __restrict__ l, const double* __restrict__ u,
+                                const double* __restrict__ x0, const double* __restrict__ y0,
+                                const double* __restrict__ dr, const double* __restrict__ dc,
+                                const uint8_t* __restrict__ is_eq, double* x, double* xa, double* xt, double* y,
+                                double* ya, double* yt, float* yg32) {
     int tid = blockIdx.x * blockDim.x + threadIdx.x, st = gridDim.x * blockDim.x;
     for (int j = tid; j < n; j += st) {
-        T v = x0s ? (T)x0s[j] : (T)0;
+        double v = x0 ? x0[j] / dc[j] : 0.0;
         v = clampT(v, l[j], u[j]);
         x[j] = v; xa[j] = v; xt[j] = v;
     }
     for (int i = tid; i < m; i += st) {
-        T v = y0s ? (T)y0s[i] : (T)0;
-        if (!is_eq[i] && v < (T)0) v = (T)0;
+        double v = y0 ? y0[i] / dr[i] : 0.0;
+        if (!is_eq[i] && v < 0.0) v = 0.0;
         y[i] = v; ya[i] = v; yt[i] = v;
+        if (yg32) yg32[i] = (float)v;
     }
-}
-
-// warm start in scaled space: x_s = x0 / dc, y_s = y0 / dr  (into temporary FP64 buffers)
-__global__ void k_warm_to_scaled(int m, int n, const double* __restrict__ dr, const double* __restrict__ dc,
-                                 double* __restrict__ x, double* __restrict__ y) {
-    int tid = blockIdx.x * blockDim.x + threadIdx.x, st = gridDim.x * blockDim.x;
-    for (int j = tid; j < n; j += st) x[j] /= dc[j];
-    for (int i = tid; i < m; i += st) y[i] /= dr[i];
 }
 
 // ------------------------------------------------------------------ iteration kernels
 enum { M_PLAIN = 0, M_FIRST = 1, M_CHECK = 2 };
 
-template <typename T>
+// VT: storage type of the matrix values and of xh (float: mixed, double: FP64).
+// GT: type of the gathered operand (primal: y, always FP64; dual: xh, VT).
+template <typename VT, typename GT>
 struct IterArgs {
-    // CSR (rows of the operator this kernel applies) and per-entry values
-    const int32_t* ptr;
+    const int32_t* ptr;    // CSR of the operator this kernel applies (A^T for primal, A for dual)
     const int32_t* idx;
-    const T* val;
-    const T* gather;     // y for the primal kernel, xh for the dual kernel
-    const T* cost;       // c (primal) / b (dual)
-    const T* lo;         // l (primal)
-    const T* hi;         // u (primal)
+    const VT* val;
+    const GT* gather;      // y for the primal kernel, xh for the dual kernel
+    const double* cost;    // c (primal) / b (dual)
+    const double* lo;      // l (primal)
+    const double* hi;      // u (primal)
     const uint8_t* is_eq;  // dual
-    T* z;                // x or y (updated in place)
-    T* zh;               // xh (primal only)
-    const T* za;         // anchor
-    T* zt;               // T(z) at check iterations
+    double* z;             // x or y, updated in place
+    VT* zh;                // primal: xh out (dual: unused)
+    const double* za;      // anchor
+    double* zt;            // T(z) at check iterations
     Ctrl* ctrl;
     int rows;
     double rho;
 };
 
-// L lanes per row; all 32 lanes of a warp stay converged through the shuffles.
-template <typename T, int L, int MODE, bool PRIMAL>
-__global__ void __launch_bounds__(TB) k_iter(IterArgs<T> a, int it) {
+// Matrix entries and row pointers are read once per iteration: bypass L1 and mark
+// them evict-first in L2, so the iterate vectors (re-read every iteration) stay
+// L2-resident while the matrix streams from HBM.
+__device__ __forceinline__ unsigned long long evict_first_policy() {
+    unsigned long long pol;
+    asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
+    return pol;
+}
+__device__ __forceinline__ float ld_stream(const float* p, unsigned long long pol) {
+    float v;
+    asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(p), "l"(pol));
+    return v;
+}
+__device__ __forceinline__ double ld_stream(const double* p, unsigned long long pol) {
+    double v;
+    asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.f64 %0, [%1], %2;" : "=d"(v) : "l"(p), "l"(pol));
+    return v;
+}
+__device__ __forceinline__ int ld_stream(const int* p, unsigned long long pol) {
+    int v;
+    asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.s32 %0, [%1], %2;" : "=r"(v) : "l"(p), "l"(pol));
+    return v;
+}
+
+// L lanes per row, R rows per lane group per step.  Within a step every load that
+// does not depend on another -- the R row-pointer pairs, the R epilogue operands,
+// the first L entries of the R rows, then their R gathers -- is issued before any
+// is consumed, so each warp keeps several independent memory requests in flight
+// (the kernel is bound by memory latency x parallelism, not by arithmetic).
+// All 32 lanes of a warp stay converged through the shuffles.  Sums and updates
+// are FP64; VT only sets the bytes streamed for values and xh.
+template <typename VT, typename GT, int L, int R, int MODE, bool PRIMAL>
+__global__ void __launch_bounds__(TB) k_iter(IterArgs<VT, GT> a, int it) {
     const Ctrl* ctrl = a.ctrl;
     if (ctrl->done) return;
+    const unsigned long long pol = evict_first_policy();
     const double kk = (double)(ctrl->k_base + it);
-    const T wk = (T)((kk + 1.0) / (kk + 2.0));
-    const T wa = (T)(1.0 / (kk + 2.0));
-    const T step = (T)(PRIMAL ? ctrl->tau : ctrl->sigma);
-    const T rho = (T)a.rho;
+    const double wk = (kk + 1.0) / (kk + 2.0);
+    const double wa = 1.0 / (kk + 2.0);
+    const double step = PRIMAL ? ctrl->tau : ctrl->sigma;
+    const double rho = a.rho;
     const int lane = threadIdx.x & 31;
     const int sub = lane & (L - 1);
-    const int rows_per_warp = 32 / L;
+    const int rpw = 32 / L;
+    const int span = rpw * R;
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int nwarps = (gridDim.x * blockDim.x) >> 5;
     double acc_r = 0.0, acc_d = 0.0;
-    for (int base = warp * rows_per_warp; base < a.rows; base += nwarps * rows_per_warp) {
-        const int r = base + lane / L;
-        const bool valid = r < a.rows;
-        T s = (T)0;
-        if (valid) {
-            const int k0 = a.ptr[r], k1 = a.ptr[r + 1];
-            for (int k = k0 + sub; k < k1; k += L) s += a.val[k] * a.gather[a.idx[k]];
+    for (int base = warp * span; base < a.rows; base += nwarps * span) {
+        int r[R], k0[R], k1[R];
+#pragma unroll
+        for (int u = 0; u < R; ++u) {
+            r[u] = base + u * rpw + lane / L;
+            const bool v = r[u] < a.rows;
+            k0[u] = v ? ld_stream(a.ptr + r[u], pol) : 0;
+            k1[u] = v ? ld_stream(a.ptr + r[u] + 1, pol) : 0;
+        }
+        double zr[R], cst[R];
+#pragma unroll
+        for (int u = 0; u < R; ++u) {
+            const bool lead = sub == 0 && r[u] < a.rows;
+            zr[u] = lead ? a.z[r[u]] : 0.0;
+            cst[u] = lead ? a.cost[r[u]] : 0.0;
+        }
+        VT v[R];
+        int c[R];
+#pragma unroll
+        for (int u = 0; u < R; ++u) {
+            const int k = k0[u] + sub;
+            const bool h = k < k1[u];
+            v[u] = h ? ld_stream(a.val + k, pol) : (VT)0;
+            c[u] = h ? ld_stream(a.idx + k, pol) : -1;
+        }
+        double s[R];
+#pragma unroll
+        for (int u = 0; u < R; ++u) s[u] = (c[u] >= 0) ? (double)v[u] * (double)a.gather[c[u]] : 0.0;
+#pragma unroll
+        for (int u = 0; u < R; ++u)
+            for (int k = k0[u] + sub + L; k < k1[u]; k += L)
+                s[u] += (double)ld_stream(a.val + k, pol) * (double)a.gather[ld_stream(a.idx + k, pol)];
+#pragma unroll
+        for (int u = 0; u < R; ++u) {
+#pragma unroll
+            for (int o = L / 2; o > 0; o >>= 1) s[u] += __shfl_xor_sync(0xffffffffu, s[u], o);
         }
 #pragma unroll
-        for (int o = L / 2; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-        if (valid && sub == 0) {
-            const T zr = a.z[r];
-            T zt;
+        for (int u = 0; u < R; ++u) {
+            if (sub != 0 || r[u] >= a.rows) continue;
+            const int row = r[u];
+            double zt;
             if (PRIMAL) {
-                zt = clampT(zr - step * (a.cost[r] + s), a.lo[r], a.hi[r]);
-                a.zh[r] = (T)2 * zt - zr;
+                zt = clampT(zr[u] - step * (cst[u] + s[u]), a.lo[row], a.hi[row]);
+                a.zh[row] = (VT)(2.0 * zt - zr[u]);
             } else {
-                zt = zr + step * (s - a.cost[r]);
-                if (!a.is_eq[r] && zt < (T)0) zt = (T)0;
+                zt = zr[u] + step * (s[u] - cst[u]);
+                if (!a.is_eq[row] && zt < 0.0) zt = 0.0;
             }
-            const T za = a.za[r];
-            a.z[r] = wk * ((T)(1) + rho) * zt - wk * rho * zr + wa * za;
+            const double za = a.za[row];
+            a.z[row] = wk * ((1.0 + rho) * zt - rho * zr[u]) + wa * za;
             if (MODE != M_PLAIN) {
-                double d = (double)zr - (double)zt;
+                const double d = zr[u] - zt;
                 acc_r += d * d;
             }
             if (MODE == M_CHECK) {
-                a.zt[r] = zt;
-                double e = (double)zt - (double)za;
+                a.zt[row] = zt;
+                const double e = zt - za;
                 acc_d += e * e;
             }
         }
@@ -301,10 +370,10 @@ __global__ void __launch_bounds__(TB) k_iter(IterArgs<T> a, int it) {
 
 // ------------------------------------------------------------------ FP64 KKT of T(z) on the original LP
 // rows: primal residual of x = dc*xt and the b.y term of y = dr*yt
-template <typename T, int L>
+template <int L>
 __global__ void __launch_bounds__(TB) k_kkt_rows(int m, const int32_t* __restrict__ ptr, const int32_t* __restrict__ idx,
-                                                 const double* __restrict__ v64, const T* __restrict__ xt,
-                                                 const T* __restrict__ yt, const double* __restrict__ b,
+                                                 const double* __restrict__ v64, const double* __restrict__ xt,
+                                                 const double* __restrict__ yt, const double* __restrict__ b,
                                                  const uint8_t* __restrict__ is_eq, const double* __restrict__ dr,
                                                  Ctrl* ctrl) {
     if (ctrl->done) return;
@@ -316,7 +385,7 @@ __global__ void __launch_bounds__(TB) k_kkt_rows(int m, const int32_t* __restric
         bool valid = r < m;
         double s = 0.0;
         if (valid)
-            for (int k = ptr[r] + sub; k < ptr[r + 1]; k += L) s += v64[k] * (double)xt[idx[k]];
+            for (int k = ptr[r] + sub; k < ptr[r + 1]; k += L) s += v64[k] * xt[idx[k]];
 #pragma unroll
         for (int o = L / 2; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
         if (valid && sub == 0) {
@@ -324,7 +393,7 @@ __global__ void __launch_bounds__(TB) k_kkt_rows(int m, const int32_t* __restric
             double rp = ax - b[r];
             if (!is_eq[r]) rp = fmax(rp, 0.0);
             p2 += rp * rp;
-            by += b[r] * (dr[r] * (double)yt[r]);
+            by += b[r] * (dr[r] * yt[r]);
         }
     }
     block_sum_to(p2, &ctrl->acc[A_PRES2]);
@@ -332,10 +401,10 @@ __global__ void __launch_bounds__(TB) k_kkt_rows(int m, const int32_t* __restric
 }
 
 // columns: reduced cost g = c + A^T y, bound multipliers lambda, dual residual, c.x and the bound terms
-template <typename T, int L>
+template <int L>
 __global__ void __launch_bounds__(TB) k_kkt_cols(int n, const int32_t* __restrict__ ptr, const int32_t* __restrict__ idx,
-                                                 const double* __restrict__ v64, const T* __restrict__ yt,
-                                                 const T* __restrict__ xt, const double* __restrict__ c,
+                                                 const double* __restrict__ v64, const double* __restrict__ yt,
+                                                 const double* __restrict__ xt, const double* __restrict__ c,
                                                  const double* __restrict__ lb, const double* __restrict__ ub,
                                                  const double* __restrict__ dc, Ctrl* ctrl) {
     if (ctrl->done) return;
@@ -347,7 +416,7 @@ __global__ void __launch_bounds__(TB) k_kkt_cols(int n, const int32_t* __restric
         bool valid = j < n;
         double s = 0.0;
         if (valid)
-            for (int k = ptr[j] + sub; k < ptr[j + 1]; k += L) s += v64[k] * (double)yt[idx[k]];
+            for (int k = ptr[j] + sub; k < ptr[j + 1]; k += L) s += v64[k] * yt[idx[k]];
 #pragma unroll
         for (int o = L / 2; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
         if (valid && sub == 0) {
@@ -356,7 +425,7 @@ __global__ void __launch_bounds__(TB) k_kkt_cols(int n, const int32_t* __restric
             double lam = (fl && fu) ? g : (fl ? fmax(g, 0.0) : (fu ? fmin(g, 0.0) : 0.0));
             double rd = g - lam;
             d2 += rd * rd;
-            double x = dc[j] * (double)xt[j];
+            double x = dc[j] * xt[j];
             pc += c[j] * x;
             if (lam > 0.0) lam_t += lam * lb[j];
             else if (lam < 0.0) lam_t += lam * ub[j];
@@ -422,24 +491,26 @@ __global__ void k_control(Ctrl* c) {
     for (int i = 0; i < A_COUNT; ++i) a[i] = 0.0;
 }
 
-// z <- z_anchor <- T(z) at a restart
-template <typename T>
-__global__ void k_restart(int m, int n, const Ctrl* __restrict__ c, T* x, T* xa, const T* __restrict__ xt, T* y, T* ya,
-                          const T* __restrict__ yt) {
+// z <- z_anchor <- T(z) at a restart (and the FP32 gather copy of y)
+__global__ void k_restart(int m, int n, const Ctrl* __restrict__ c, double* x, double* xa, const double* __restrict__ xt,
+                          double* y, double* ya, const double* __restrict__ yt, float* yg32) {
     if (c->done || !c->restart) return;
     int tid = blockIdx.x * blockDim.x + threadIdx.x, st = gridDim.x * blockDim.x;
-    for (int j = tid; j < n; j += st) { T v = xt[j]; x[j] = v; xa[j] = v; }
-    for (int i = tid; i < m; i += st) { T v = yt[i]; y[i] = v; ya[i] = v; }
+    for (int j = tid; j < n; j += st) { double v = xt[j]; x[j] = v; xa[j] = v; }
+    for (int i = tid; i < m; i += st) {
+        double v = yt[i];
+        y[i] = v; ya[i] = v;
+        if (yg32) yg32[i] = (float)v;
+    }
 }
 
 // unscale T(z) into FP64 outputs: x = dc * xt, y = dr * yt
-template <typename T>
-__global__ void k_unscale(int m, int n, const T* __restrict__ xt, const T* __restrict__ yt,
+__global__ void k_unscale(int m, int n, const double* __restrict__ xt, const double* __restrict__ yt,
                           const double* __restrict__ dr, const double* __restrict__ dc, double* __restrict__ xo,
                           double* __restrict__ yo) {
     int tid = blockIdx.x * blockDim.x + threadIdx.x, st = gridDim.x * blockDim.x;
-    for (int j = tid; j < n; j += st) xo[j] = dc[j] * (double)xt[j];
-    for (int i = tid; i < m; i += st) yo[i] = dr[i] * (double)yt[i];
+    for (int j = tid; j < n; j += st) xo[j] = dc[j] * xt[j];
+    for (int i = tid; i < m; i += st) yo[i] = dr[i] * yt[i];
 }
 
 int pick_lanes(double mean_len, int requested) {
@@ -450,37 +521,32 @@ int pick_lanes(double mean_len, int requested) {
     return L;
 }
 
-template <typename T, int MODE, bool PRIMAL>
-void launch_iter_L(int L, unsigned grid, cudaStream_t s, const IterArgs<T>& a, int it) {
+template <typename VT, typename GT, int R, int MODE, bool PRIMAL>
+void launch_iter_LR(int L, unsigned grid, cudaStream_t s, const IterArgs<VT, GT>& a, int it) {
     switch (L) {
-        case 2: k_iter<T, 2, MODE, PRIMAL><<<grid, TB, 0, s>>>(a, it); break;
-        case 4: k_iter<T, 4, MODE, PRIMAL><<<grid, TB, 0, s>>>(a, it); break;
-        case 8: k_iter<T, 8, MODE, PRIMAL><<<grid, TB, 0, s>>>(a, it); break;
-        case 16: k_iter<T, 16, MODE, PRIMAL><<<grid, TB, 0, s>>>(a, it); break;
-        default: k_iter<T, 32, MODE, PRIMAL><<<grid, TB, 0, s>>>(a, it); break;
+        case 2: k_iter<VT, GT, 2, R, MODE, PRIMAL><<<grid, TB, 0, s>>>(a, it); break;
+        case 4: k_iter<VT, GT, 4, R, MODE, PRIMAL><<<grid, TB, 0, s>>>(a, it); break;
+        case 8: k_iter<VT, GT, 8, R, MODE, PRIMAL><<<grid, TB, 0, s>>>(a, it); break;
+        case 16: k_iter<VT, GT, 16, R, MODE, PRIMAL><<<grid, TB, 0, s>>>(a, it); break;
+        default: k_iter<VT, GT, 32, R, MODE, PRIMAL><<<grid, TB, 0, s>>>(a, it); break;
     }
 }
 
-template <typename T>
-void launch_iter(int mode, bool primal, int L, unsigned grid, cudaStream_t s, const IterArgs<T>& a, int it) {
-    if (primal) {
-        if (mode == M_PLAIN) launch_iter_L<T, M_PLAIN, true>(L, grid, s, a, it);
-        else if (mode == M_FIRST) launch_iter_L<T, M_FIRST, true>(L, grid, s, a, it);
-        else launch_iter_L<T, M_CHECK, true>(L, grid, s, a, it);
-    } else {
-        if (mode == M_PLAIN) launch_iter_L<T, M_PLAIN, false>(L, grid, s, a, it);
-        else if (mode == M_FIRST) launch_iter_L<T, M_FIRST, false>(L, grid, s, a, it);
-        else launch_iter_L<T, M_CHECK, false>(L, grid, s, a, it);
-    }
+// Plain iterations use R rows per lane group; the two reduction iterations of a chunk use R = 1.
+template <typename VT, typename GT, bool PRIMAL>
+void launch_iter(int mode, int L, int R, unsigned grid, cudaStream_t s, const IterArgs<VT, GT>& a, int it) {
+    if (mode == M_FIRST) launch_iter_LR<VT, GT, 1, M_FIRST, PRIMAL>(L, grid, s, a, it);
+    else if (mode == M_CHECK) launch_iter_LR<VT, GT, 1, M_CHECK, PRIMAL>(L, grid, s, a, it);
+    else if (R >= 4) launch_iter_LR<VT, GT, 4, M_PLAIN, PRIMAL>(L, grid, s, a, it);
+    else if (R == 2) launch_iter_LR<VT, GT, 2, M_PLAIN, PRIMAL>(L, grid, s, a, it);
+    else launch_iter_LR<VT, GT, 1, M_PLAIN, PRIMAL>(L, grid, s, a, it);
 }
 
-template <typename T>
-void launch_kkt(int Lr, int Lc, unsigned gr, unsigned gc, cudaStream_t s, const DevLP& lp, HalpernWork* w,
-                const T* xt, const T* yt, Ctrl* ctrl) {
-#define KR(LL) k_kkt_rows<T, LL><<<gr, TB, 0, s>>>(lp.m, lp.rowptr.p, lp.colidx.p, w->sv64.p, xt, yt, lp.b.p, lp.is_eq.p, w->dr.p, ctrl)
-#define KC(LL) k_kkt_cols<T, LL><<<gc, TB, 0, s>>>(lp.n, lp.t_rowptr.p, lp.t_colidx.p, w->stv64.p, yt, xt, lp.c.p, lp.lb.p, lp.ub.p, w->dc.p, ctrl)
-    switch (Lr) { case 2: KR(2); break; case 4: KR(4); break; case 8: KR(8); break; case 16: KR(16); break; default: KR(32); }
-    switch (Lc) { case 2: KC(2); break; case 4: KC(4); break; case 8: KC(8); break; case 16: KC(16); break; default: KC(32); }
+void launch_kkt(int Lr, int Lc, unsigned gr, unsigned gc, cudaStream_t s, const DevLP& lp, HalpernWork* w, Ctrl* ctrl) {
+#define KR(LL) k_kkt_rows<LL><<<gr, TB, 0, s>>>(lp.m, lp.rowptr.p, lp.colidx.p, w->sv64.p, w->xt.p, w->yt.p, lp.b.p, lp.is_eq.p, w->dr.p, ctrl)
+#define KC(LL) k_kkt_cols<LL><<<gc, TB, 0, s>>>(lp.n, lp.t_rowptr.p, lp.t_colidx.p, w->stv64.p, w->yt.p, w->xt.p, lp.c.p, lp.lb.p, lp.ub.p, w->dc.p, ctrl)
+    switch (Lr) { case 1: KR(1); break; case 2: KR(2); break; case 4: KR(4); break; case 8: KR(8); break; case 16: KR(16); break; default: KR(32); }
+    switch (Lc) { case 1: KC(1); break; case 2: KC(2); break; case 4: KC(4); break; case 8: KC(8); break; case 16: KC(16); break; default: KC(32); }
 #undef KR
 #undef KC
 }
@@ -510,8 +576,7 @@ int prepare_scaling(Ctx* ctx, HalpernWork* w, int ruiz_iters, bool need32) {
                                    need32 ? w->stv32.p : nullptr);
     unsigned gmn = grid_for(std::max(m, n), TB, ctx->sm_count);
     k_scale_vecs<<<gmn, TB, 0, s>>>(m, n, L.b.p, L.c.p, L.lb.p, L.ub.p, w->dr.p, w->dc.p, w->b64.p, w->c64.p, w->l64.p,
-                                    w->u64.p, need32 ? w->b32.p : nullptr, need32 ? w->c32.p : nullptr,
-                                    need32 ? w->l32.p : nullptr, need32 ? w->u32.p : nullptr);
+                                    w->u64.p, nullptr, nullptr, nullptr, nullptr);
     B2P_LAUNCH(ctx);
     ctx->launches += 4 * ruiz_iters + 7;
     return B2P_OK;
@@ -523,21 +588,13 @@ int power_sigma2(Ctx* ctx, HalpernWork* w, double* sigma2) {
     cudaStream_t s = ctx->stream;
     const int m = L.m, n = L.n;
     unsigned gm = grid_for(m, TB, ctx->sm_count), gn = grid_for(n, TB, ctx->sm_count, 4);
-    double* scal = w->pw.p;  // [0] nrm2 accumulator, [1] nv, [2..] history
+    double* scal = w->pw.p;  // [0] ||w||^2 accumulator, [1] ||v||, [2..17] history of ||A^T A v|| / ||v||
     const int kMax = 512, kRound = 16;
     k_pow_init<<<gn, TB, 0, s>>>(n, w->pv.p);
     k_fill<<<1, 32, 0, s>>>(2, 0.0, scal);
-    double one = 1.0;
-    B2P_CUDA(ctx, cudaMemcpyAsync(scal + 1, &one, sizeof(double), cudaMemcpyHostToDevice, s));
-    // normalise the start vector: one pass with u = A v and w = A^T u is not needed; instead
-    // take its norm through the first round's history (the estimate uses ||A^T A v|| / ||v||).
-    double hist[kRound];
-    double prev = 0.0, est = 0.0;
-    // first: make v unit length using a column pass on itself
+    B2P_LAUNCH(ctx);
+    // ||v|| of the start vector (once, on the host)
     {
-        // ||v||^2 via k_pow_cols with identity-free trick: compute once on host-visible path
-        DBuf<double> tmp;
-        B2P_CUDA(ctx, tmp.reserve(n));
         std::vector<double> hv(n);
         B2P_CUDA(ctx, cudaMemcpyAsync(hv.data(), w->pv.p, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
         B2P_CUDA(ctx, cudaStreamSynchronize(s));
@@ -546,10 +603,10 @@ int power_sigma2(Ctx* ctx, HalpernWork* w, double* sigma2) {
         nn = std::sqrt(nn);
         B2P_CUDA(ctx, cudaMemcpyAsync(scal + 1, &nn, sizeof(double), cudaMemcpyHostToDevice, s));
     }
-    int t = 0;
-    for (; t < kMax; t += kRound) {
+    double hist[kRound];
+    double est = 0.0;
+    for (int t = 0; t < kMax; t += kRound) {
         for (int q = 0; q < kRound; ++q) {
-            // v enters normalised by scal[1]; u = A v / ||v|| ; w = A^T u ; ||w|| -> sigma^2 estimate
             k_pow_rows<<<gm, TB, 0, s>>>(m, L.rowptr.p, L.colidx.p, w->sv64.p, w->pv.p, scal + 1, w->pu.p);
             k_pow_cols<<<gn, TB, 0, s>>>(n, L.t_rowptr.p, L.t_colidx.p, w->stv64.p, w->pu.p, w->pv.p, scal);
             k_pow_finish<<<1, 1, 0, s>>>(scal, scal + 1, scal + 2, q);
@@ -559,41 +616,126 @@ int power_sigma2(Ctx* ctx, HalpernWork* w, double* sigma2) {
         B2P_CUDA(ctx, cudaMemcpyAsync(hist, scal + 2, sizeof(hist), cudaMemcpyDeviceToHost, s));
         B2P_CUDA(ctx, cudaStreamSynchronize(s));
         est = hist[kRound - 1];
-        prev = hist[kRound - 2];
+        double prev = hist[kRound - 2];
         if (est > 0 && std::fabs(est - prev) <= 1e-7 * est) break;
     }
     *sigma2 = est;
     return B2P_OK;
 }
 
-template <typename T>
-struct Bufs {
-    T *x, *xh, *xa, *xt, *y, *ya, *yt, *c, *b, *l, *u;
-    const T *sv, *stv;
+template <typename MT>
+struct Ops;
+template <>
+struct Ops<double> {
+    static const double* sv(HalpernWork* w) { return w->sv64.p; }
+    static const double* stv(HalpernWork* w) { return w->stv64.p; }
+    static double* xh(HalpernWork* w) { return w->xh64.p; }
+};
+template <>
+struct Ops<float> {
+    static const float* sv(HalpernWork* w) { return w->sv32.p; }
+    static const float* stv(HalpernWork* w) { return w->stv32.p; }
+    static float* xh(HalpernWork* w) { return w->xh32.p; }
 };
 
-template <typename T>
-int run_chunks(Ctx* ctx, HalpernWork* w, const b2p_params* p, Bufs<T> B, double time_limit_ms, double t_start) {
+inline unsigned iter_grid(int64_t rows, int L, int R, int sm_count) {
+    return grid_for((rows * L + R - 1) / R, TB, sm_count, 8);
+}
+
+// Times candidate (L, R) launch shapes of the primal and dual kernels on the
+// uploaded LP (plain iterations from the current iterates, CUDA events on the
+// context stream) and keeps the fastest of each.  The caller re-initialises the
+// iterates afterwards.  Explicit lanes_per_row skips the search.
+template <typename MT>
+int autotune_shapes(Ctx* ctx, HalpernWork* w, const b2p_params* p) {
+    DevLP& L = ctx->lp;
+    const long long key = ((long long)L.nnz * 1000003LL + (long long)L.m * 101LL + L.n) * 2 + (sizeof(MT) == 4);
+    if (p->lanes_per_row > 0) {
+        w->Lc = w->Lr = pick_lanes(0, p->lanes_per_row);
+        w->Rc = w->Rr = 1;
+        w->tuned_key = -1;
+        return B2P_OK;
+    }
+    if (w->tuned_key == key) return B2P_OK;
+    cudaStream_t s = ctx->stream;
+    const int m = L.m, n = L.n;
+    Ctrl* ctrl = w->ctrl.p;
+    IterArgs<MT, double> pa{L.t_rowptr.p, L.t_colidx.p, Ops<MT>::stv(w), w->y.p, w->c64.p, w->l64.p, w->u64.p,
+                            nullptr, w->x.p, Ops<MT>::xh(w), w->xa.p, w->xt.p, ctrl, n, p->reflection};
+    IterArgs<MT, MT> da{L.rowptr.p, L.colidx.p, Ops<MT>::sv(w), Ops<MT>::xh(w), w->b64.p, nullptr, nullptr, L.is_eq.p,
+                        w->y.p, nullptr, w->ya.p, w->yt.p, ctrl, m, p->reflection};
+    cudaEvent_t e0, e1;
+    B2P_CUDA(ctx, cudaEventCreate(&e0));
+    B2P_CUDA(ctx, cudaEventCreate(&e1));
+    for (int side = 0; side < 2; ++side) {
+        const bool primal = side == 0;
+        const double mean = primal ? L.mean_col_len : L.mean_row_len;
+        const int base_L = pick_lanes(mean, 0);
+        float best = 1e30f;
+        int bestL = base_L, bestR = 1;
+        for (int Lc : {base_L / 2, base_L, base_L * 2}) {
+            if (Lc < 2 || Lc > 32) continue;
+            for (int R : {1, 2, 4}) {
+                const int64_t rows = primal ? n : m;
+                unsigned g = iter_grid(rows, Lc, R, ctx->sm_count);
+                float tot = 0.f;
+                for (int rep = 0; rep < 4; ++rep) {
+                    cudaEventRecord(e0, s);
+                    if (primal) launch_iter<MT, double, true>(M_PLAIN, Lc, R, g, s, pa, rep);
+                    else launch_iter<MT, MT, false>(M_PLAIN, Lc, R, g, s, da, rep);
+                    cudaEventRecord(e1, s);
+                    B2P_LAUNCH(ctx);
+                    B2P_CUDA(ctx, cudaEventSynchronize(e1));
+                    float ms = 0.f;
+                    cudaEventElapsedTime(&ms, e0, e1);
+                    if (rep > 0) tot += ms;  // first launch warms caches
+                }
+                ctx->launches += 4;
+                if (tot < best) {
+                    best = tot;
+                    bestL = Lc;
+                    bestR = R;
+                }
+            }
+        }
+        if (primal) { w->Lc = bestL; w->Rc = bestR; }
+        else { w->Lr = bestL; w->Rr = bestR; }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    w->tuned_key = key;
+    return B2P_OK;
+}
+
+template <typename MT>
+int run_chunks(Ctx* ctx, HalpernWork* w, const b2p_params* p, double time_limit_ms, double t_start) {
     DevLP& L = ctx->lp;
     cudaStream_t s = ctx->stream;
     const int m = L.m, n = L.n, K = p->check_every;
-    int Lr = pick_lanes(L.mean_row_len, p->lanes_per_row);
-    int Lc = pick_lanes(L.mean_col_len, p->lanes_per_row);
-    // rows handled per warp = 32 / L ; enough warps to cover all rows, capped at 8 CTAs per SM
-    unsigned gr = grid_for((int64_t)m * Lr, TB, ctx->sm_count, 8);
-    unsigned gc = grid_for((int64_t)n * Lc, TB, ctx->sm_count, 8);
+    const int Lr = w->Lr, Lc = w->Lc, Rr = w->Rr, Rc = w->Rc;
+    // R = 1 grids serve the reduction iterations and the KKT kernels
+    unsigned gr = iter_grid(m, Lr, 1, ctx->sm_count), gc = iter_grid(n, Lc, 1, ctx->sm_count);
+    unsigned grR = iter_grid(m, Lr, Rr, ctx->sm_count), gcR = iter_grid(n, Lc, Rc, ctx->sm_count);
     Ctrl* ctrl = w->ctrl.p;
-    IterArgs<T> pa{L.t_rowptr.p, L.t_colidx.p, B.stv, B.y, B.c, B.l, B.u, nullptr, B.x, B.xh, B.xa, B.xt, ctrl, n, p->reflection};
-    IterArgs<T> da{L.rowptr.p, L.colidx.p, B.sv, B.xh, B.b, nullptr, nullptr, L.is_eq.p, B.y, nullptr, B.ya, B.yt, ctrl, m, p->reflection};
+    IterArgs<MT, double> pa{L.t_rowptr.p, L.t_colidx.p, Ops<MT>::stv(w), w->y.p, w->c64.p, w->l64.p, w->u64.p,
+                            nullptr, w->x.p, Ops<MT>::xh(w), w->xa.p, w->xt.p, ctrl, n, p->reflection};
+    IterArgs<MT, MT> da{L.rowptr.p, L.colidx.p, Ops<MT>::sv(w), Ops<MT>::xh(w), w->b64.p, nullptr, nullptr, L.is_eq.p,
+                        w->y.p, nullptr, w->ya.p, w->yt.p, ctrl, m, p->reflection};
     auto chunk = [&]() {
         for (int i = 0; i < K; ++i) {
             int mode = (i == 0) ? M_FIRST : (i == K - 1 ? M_CHECK : M_PLAIN);
-            launch_iter<T>(mode, true, Lc, gc, s, pa, i);
-            launch_iter<T>(mode, false, Lr, gr, s, da, i);
+            if (mode == M_PLAIN) {
+                launch_iter<MT, double, true>(mode, Lc, Rc, gcR, s, pa, i);
+                launch_iter<MT, MT, false>(mode, Lr, Rr, grR, s, da, i);
+            } else {
+                launch_iter<MT, double, true>(mode, Lc, 1, gc, s, pa, i);
+                launch_iter<MT, MT, false>(mode, Lr, 1, gr, s, da, i);
+            }
         }
-        launch_kkt<T>(Lr, Lc, gr, gc, s, L, w, B.xt, B.yt, ctrl);
+        launch_kkt(Lr, Lc, gr, gc, s, L, w, ctrl);
         k_control<<<1, 1, 0, s>>>(ctrl);
-        k_restart<T><<<grid_for(std::max(m, n), TB, ctx->sm_count, 8), TB, 0, s>>>(m, n, ctrl, B.x, B.xa, B.xt, B.y, B.ya, B.yt);
+        k_restart<<<grid_for(std::max(m, n), TB, ctx->sm_count, 8), TB, 0, s>>>(m, n, ctrl, w->x.p, w->xa.p, w->xt.p,
+                                                                               w->y.p, w->ya.p, w->yt.p, nullptr);
     };
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
@@ -610,7 +752,7 @@ int run_chunks(Ctx* ctx, HalpernWork* w, const b2p_params* p, Bufs<T> B, double 
         ctx->err = std::string("graph instantiate: ") + cudaGetErrorString(ce);
         return B2P_EXECUTION_FAILED;
     }
-    const int64_t per_chunk = 2 * K + 5;
+    const int64_t per_chunk = 2 * K + 4;
     int64_t launched = 0;
     int slot = 0;
     bool timed_out = false;
@@ -647,58 +789,30 @@ int run_chunks(Ctx* ctx, HalpernWork* w, const b2p_params* p, Bufs<T> B, double 
     return timed_out ? B2P_TIMEOUT : B2P_OK;
 }
 
-template <typename T>
-Bufs<T> bufs_of(HalpernWork* w);
-template <>
-Bufs<double> bufs_of<double>(HalpernWork* w) {
-    return {w->x64.p, w->xh64.p, w->xa64.p, w->xt64.p, w->y64.p, w->ya64.p, w->yt64.p,
-            w->c64.p, w->b64.p, w->l64.p, w->u64.p, w->sv64.p, w->stv64.p};
-}
-template <>
-Bufs<float> bufs_of<float>(HalpernWork* w) {
-    return {w->x32.p, w->xh32.p, w->xa32.p, w->xt32.p, w->y32.p, w->ya32.p, w->yt32.p,
-            w->c32.p, w->b32.p, w->l32.p, w->u32.p, w->sv32.p, w->stv32.p};
-}
-
-template <typename T>
-int alloc_iterates(Ctx* ctx, HalpernWork* w);
-template <>
-int alloc_iterates<double>(Ctx* ctx, HalpernWork* w) {
-    int m = ctx->lp.m, n = ctx->lp.n;
-    for (auto* b : {&w->x64, &w->xh64, &w->xa64, &w->xt64}) B2P_CUDA(ctx, b->reserve(n));
-    for (auto* b : {&w->y64, &w->ya64, &w->yt64}) B2P_CUDA(ctx, b->reserve(m));
-    return B2P_OK;
-}
-template <>
-int alloc_iterates<float>(Ctx* ctx, HalpernWork* w) {
-    int m = ctx->lp.m, n = ctx->lp.n;
-    int64_t nnz = ctx->lp.nnz;
-    for (auto* b : {&w->x32, &w->xh32, &w->xa32, &w->xt32, &w->c32, &w->l32, &w->u32}) B2P_CUDA(ctx, b->reserve(n));
-    for (auto* b : {&w->y32, &w->ya32, &w->yt32, &w->b32}) B2P_CUDA(ctx, b->reserve(m));
-    B2P_CUDA(ctx, w->sv32.reserve(nnz));
-    B2P_CUDA(ctx, w->stv32.reserve(nnz));
-    return B2P_OK;
-}
-
-template <typename T>
+template <typename MT>
 int solve_T(Ctx* ctx, HalpernWork* w, const b2p_params* p, const double* x0, const double* y0, b2p_result* r,
             double* x_out, double* y_out) {
     DevLP& L = ctx->lp;
     cudaStream_t s = ctx->stream;
     const int m = L.m, n = L.n;
+    const bool mixed = sizeof(MT) == 4;
     double t_start = now_ms();
-    int st = alloc_iterates<T>(ctx, w);
-    if (st) return st;
-    st = prepare_scaling(ctx, w, p->ruiz_iterations, sizeof(T) == 4);
+    if (mixed) {
+        B2P_CUDA(ctx, w->xh32.reserve(n));
+        B2P_CUDA(ctx, w->sv32.reserve(L.nnz));
+        B2P_CUDA(ctx, w->stv32.reserve(L.nnz));
+    } else {
+        B2P_CUDA(ctx, w->xh64.reserve(n));
+    }
+    int st = prepare_scaling(ctx, w, p->ruiz_iterations, mixed);
     if (st) return st;
     double sig2 = 0.0;
     st = power_sigma2(ctx, w, &sig2);
     if (st) return st;
     double sigma_max = std::sqrt(std::max(sig2, 0.0));
     double eta = sigma_max > 0 ? p->step_safety / sigma_max : 1.0;
-    // primal weight ||c_s|| / ||b_s||
     double omega = p->primal_weight;
-    if (!(omega > 0)) {
+    if (!(omega > 0)) {  // ||c_s|| / ||b_s||
         std::vector<double> hb(m), hc(n);
         B2P_CUDA(ctx, cudaMemcpyAsync(hb.data(), w->b64.p, sizeof(double) * m, cudaMemcpyDeviceToHost, s));
         B2P_CUDA(ctx, cudaMemcpyAsync(hc.data(), w->c64.p, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
@@ -710,25 +824,22 @@ int solve_T(Ctx* ctx, HalpernWork* w, const b2p_params* p, const double* x0, con
         cn = std::sqrt(cn);
         omega = (bn > 1e-10 && cn > 1e-10) ? cn / bn : 1.0;
     }
-    Bufs<T> B = bufs_of<T>(w);
-    // warm start (original space) -> scaled FP64 temporaries
-    double* x0s = nullptr;
-    double* y0s = nullptr;
-    if (x0 || y0) {
-        B2P_CUDA(ctx, w->tmp_n.reserve(n));
-        B2P_CUDA(ctx, w->tmp_m.reserve(m));
-        if (x0) B2P_CUDA(ctx, cudaMemcpyAsync(w->tmp_n.p, x0, sizeof(double) * n, cudaMemcpyHostToDevice, s));
-        else B2P_CUDA(ctx, cudaMemsetAsync(w->tmp_n.p, 0, sizeof(double) * n, s));
-        if (y0) B2P_CUDA(ctx, cudaMemcpyAsync(w->tmp_m.p, y0, sizeof(double) * m, cudaMemcpyHostToDevice, s));
-        else B2P_CUDA(ctx, cudaMemsetAsync(w->tmp_m.p, 0, sizeof(double) * m, s));
-        k_warm_to_scaled<<<grid_for(std::max(m, n), TB, ctx->sm_count), TB, 0, s>>>(m, n, w->dr.p, w->dc.p, w->tmp_n.p, w->tmp_m.p);
-        x0s = w->tmp_n.p;
-        y0s = w->tmp_m.p;
+    // warm start (original space) -> device temporaries
+    const double* x0d = nullptr;
+    const double* y0d = nullptr;
+    if (x0) {
+        B2P_CUDA(ctx, cudaMemcpyAsync(w->tmp_n.p, x0, sizeof(double) * n, cudaMemcpyHostToDevice, s));
+        x0d = w->tmp_n.p;
     }
-    k_init_iterates<T><<<grid_for(std::max(m, n), TB, ctx->sm_count), TB, 0, s>>>(m, n, B.l, B.u, x0s, y0s, L.is_eq.p,
-                                                                                  B.x, B.xa, B.xt, B.y, B.ya, B.yt);
+    if (y0) {
+        B2P_CUDA(ctx, cudaMemcpyAsync(w->tmp_m.p, y0, sizeof(double) * m, cudaMemcpyHostToDevice, s));
+        y0d = w->tmp_m.p;
+    }
+    k_init_iterates<<<grid_for(std::max(m, n), TB, ctx->sm_count), TB, 0, s>>>(
+        m, n, w->l64.p, w->u64.p, x0d, y0d, w->dr.p, w->dc.p, L.is_eq.p, w->x.p, w->xa.p, w->xt.p, w->y.p, w->ya.p,
+        w->yt.p, nullptr);
     B2P_LAUNCH(ctx);
-    ctx->launches += 2;
+    ctx->launches += 1;
     Ctrl hc;
     std::memset(&hc, 0, sizeof(hc));
     hc.omega = omega;
@@ -746,8 +857,21 @@ int solve_T(Ctx* ctx, HalpernWork* w, const b2p_params* p, const double* x0, con
     hc.first_after_restart = 1;
     hc.status = B2P_STATUS_MAX_ITERATIONS;
     B2P_CUDA(ctx, cudaMemcpyAsync(w->ctrl.p, &hc, sizeof(Ctrl), cudaMemcpyHostToDevice, s));
+    {
+        const long long before = w->tuned_key;
+        st = autotune_shapes<MT>(ctx, w, p);  // returns at once when this LP shape is already tuned
+        if (st) return st;
+        if (before != w->tuned_key && w->tuned_key >= 0) {  // the trial iterations moved the iterates: reset
+            k_init_iterates<<<grid_for(std::max(m, n), TB, ctx->sm_count), TB, 0, s>>>(
+                m, n, w->l64.p, w->u64.p, x0d, y0d, w->dr.p, w->dc.p, L.is_eq.p, w->x.p, w->xa.p, w->xt.p, w->y.p,
+                w->ya.p, w->yt.p, nullptr);
+            B2P_LAUNCH(ctx);
+            ctx->launches += 1;
+            B2P_CUDA(ctx, cudaMemcpyAsync(w->ctrl.p, &hc, sizeof(Ctrl), cudaMemcpyHostToDevice, s));
+        }
+    }
     B2P_CUDA(ctx, cudaEventRecord(ctx->ev0, s));
-    st = run_chunks<T>(ctx, w, p, B, p->time_limit_s * 1000.0, t_start);
+    st = run_chunks<MT>(ctx, w, p, p->time_limit_s * 1000.0, t_start);
     B2P_CUDA(ctx, cudaEventRecord(ctx->ev1, s));
     if (st != B2P_OK && st != B2P_TIMEOUT) return st;
     Ctrl fin;
@@ -769,10 +893,8 @@ int solve_T(Ctx* ctx, HalpernWork* w, const b2p_params* p, const double* x0, con
     r->step_size = eta;
     if (x_out || y_out) {
         double t0 = now_ms();
-        B2P_CUDA(ctx, w->tmp_n.reserve(n));
-        B2P_CUDA(ctx, w->tmp_m.reserve(m));
-        k_unscale<T><<<grid_for(std::max(m, n), TB, ctx->sm_count), TB, 0, s>>>(m, n, B.xt, B.yt, w->dr.p, w->dc.p,
-                                                                               w->tmp_n.p, w->tmp_m.p);
+        k_unscale<<<grid_for(std::max(m, n), TB, ctx->sm_count), TB, 0, s>>>(m, n, w->xt.p, w->yt.p, w->dr.p, w->dc.p,
+                                                                           w->tmp_n.p, w->tmp_m.p);
         B2P_LAUNCH(ctx);
         ctx->launches += 1;
         if (x_out) B2P_CUDA(ctx, cudaMemcpyAsync(x_out, w->tmp_n.p, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
@@ -783,7 +905,76 @@ int solve_T(Ctx* ctx, HalpernWork* w, const b2p_params* p, const double* x0, con
     return B2P_OK;
 }
 
+template <typename MT>
+int kernel_timing_T(Ctx* ctx, HalpernWork* w, const b2p_params* p, int reps, double* pms, double* dms, double* pb,
+                    double* db) {
+    DevLP& L = ctx->lp;
+    cudaStream_t s = ctx->stream;
+    const int m = L.m, n = L.n;
+    const int Lr = w->Lr, Lc = w->Lc, Rr = w->Rr, Rc = w->Rc;
+    unsigned gr = iter_grid(m, Lr, Rr, ctx->sm_count), gc = iter_grid(n, Lc, Rc, ctx->sm_count);
+    Ctrl* ctrl = w->ctrl.p;
+    // re-open the (finished) control block for plain iterations, restore it afterwards
+    Ctrl saved;
+    B2P_CUDA(ctx, cudaMemcpyAsync(&saved, ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, s));
+    B2P_CUDA(ctx, cudaStreamSynchronize(s));
+    Ctrl open = saved;
+    open.done = 0;
+    B2P_CUDA(ctx, cudaMemcpyAsync(ctrl, &open, sizeof(Ctrl), cudaMemcpyHostToDevice, s));
+    IterArgs<MT, double> pa{L.t_rowptr.p, L.t_colidx.p, Ops<MT>::stv(w), w->y.p, w->c64.p, w->l64.p, w->u64.p,
+                            nullptr, w->x.p, Ops<MT>::xh(w), w->xa.p, w->xt.p, ctrl, n, p->reflection};
+    IterArgs<MT, MT> da{L.rowptr.p, L.colidx.p, Ops<MT>::sv(w), Ops<MT>::xh(w), w->b64.p, nullptr, nullptr, L.is_eq.p,
+                        w->y.p, nullptr, w->ya.p, w->yt.p, ctrl, m, p->reflection};
+    cudaEvent_t e[3];
+    for (auto& x : e) B2P_CUDA(ctx, cudaEventCreate(&x));
+    double tp = 0, td = 0;
+    for (int r = 0; r < reps; ++r) {
+        cudaEventRecord(e[0], s);
+        launch_iter<MT, double, true>(M_PLAIN, Lc, Rc, gc, s, pa, r);
+        cudaEventRecord(e[1], s);
+        launch_iter<MT, MT, false>(M_PLAIN, Lr, Rr, gr, s, da, r);
+        cudaEventRecord(e[2], s);
+        B2P_LAUNCH(ctx);
+        B2P_CUDA(ctx, cudaEventSynchronize(e[2]));
+        float a = 0, b = 0;
+        cudaEventElapsedTime(&a, e[0], e[1]);
+        cudaEventElapsedTime(&b, e[1], e[2]);
+        tp += a;
+        td += b;
+    }
+    ctx->launches += 2LL * reps;
+    for (auto& x : e) cudaEventDestroy(x);
+    B2P_CUDA(ctx, cudaMemcpyAsync(ctrl, &saved, sizeof(Ctrl), cudaMemcpyHostToDevice, s));
+    B2P_CUDA(ctx, cudaStreamSynchronize(s));
+    *pms = tp / reps;
+    *dms = td / reps;
+    // algorithmic bytes: every matrix entry, row pointer and vector element once
+    const double vb = sizeof(MT), nnz = (double)L.nnz;
+    // primal: A^T values+indices, col pointers, gather y (m x 8), x r/w, xa, c, l, u (8 each), xh write
+    *pb = nnz * (vb + 4) + 4.0 * (n + 1) + 8.0 * m + n * (8 * 6 + vb);
+    // dual: A values+indices, row pointers, gather xh (n x vb), y r/w, ya, b (8 each), is_eq (1)
+    *db = nnz * (vb + 4) + 4.0 * (m + 1) + vb * n + m * (8 * 4 + 1);
+    return B2P_OK;
+}
+
 }  // namespace
+
+int halpern_kernel_timing(Ctx* ctx, const b2p_params* p, int reps, double* primal_ms, double* dual_ms,
+                          double* primal_bytes, double* dual_bytes) {
+    HalpernWork* w = ctx->hw;
+    if (p->precision == B2P_FP32) {
+        if (!w->xh32.p || !w->sv32.p) {
+            ctx->err = "b2p_kernel_timing: no mixed-precision solve to time";
+            return B2P_NO_LP;
+        }
+        return kernel_timing_T<float>(ctx, w, p, reps, primal_ms, dual_ms, primal_bytes, dual_bytes);
+    }
+    if (!w->xh64.p) {
+        ctx->err = "b2p_kernel_timing: no FP64 solve to time";
+        return B2P_NO_LP;
+    }
+    return kernel_timing_T<double>(ctx, w, p, reps, primal_ms, dual_ms, primal_bytes, dual_bytes);
+}
 
 int halpern_engine_solve(Ctx* ctx, const b2p_params* p, const double* x0, const double* y0, b2p_result* r,
                          double* x_out, double* y_out) {
@@ -800,12 +991,11 @@ int halpern_engine_solve(Ctx* ctx, const b2p_params* p, const double* x0, const 
     HalpernWork* w = ctx->hw;
     const int m = L.m, n = L.n;
     const int64_t nnz = L.nnz;
-    if (w->m != m || w->n != n) {
-        w->m = m;
-        w->n = n;
-    }
-    for (auto* b : {&w->dc, &w->tmp_n, &w->pv, &w->c64, &w->l64, &w->u64}) B2P_CUDA(ctx, b->reserve(n));
-    for (auto* b : {&w->dr, &w->tmp_m, &w->pu, &w->b64}) B2P_CUDA(ctx, b->reserve(m));
+    w->m = m;
+    w->n = n;
+    for (auto* b : {&w->dc, &w->tmp_n, &w->pv, &w->c64, &w->l64, &w->u64, &w->x, &w->xa, &w->xt})
+        B2P_CUDA(ctx, b->reserve(n));
+    for (auto* b : {&w->dr, &w->tmp_m, &w->pu, &w->b64, &w->y, &w->ya, &w->yt}) B2P_CUDA(ctx, b->reserve(m));
     B2P_CUDA(ctx, w->pw.reserve(64));
     B2P_CUDA(ctx, w->sv64.reserve(nnz));
     B2P_CUDA(ctx, w->stv64.reserve(nnz));

@@ -125,8 +125,10 @@ def _distinct_rows_per_column(rng: np.random.Generator, m: int, n: int, k: np.nd
     idx = np.argsort(keys, axis=1)
     s = np.take_along_axis(s, idx, axis=1)
     ok = np.take_along_axis(~dup, idx, axis=1)
-    if not np.all(ok.sum(axis=1) >= k):   # pragma: no cover - vanishingly rare for the sizes used
-        raise RuntimeError("not enough distinct rows; increase candidate pool")
+    # columns whose candidate pool held fewer than k_j distinct rows (small m): draw those
+    # columns again without replacement, one by one
+    for j in np.nonzero(ok.sum(axis=1) < k)[0]:
+        s[j, :k[j]] = np.sort(rng.choice(m, size=int(k[j]), replace=False))
     take = np.arange(kmax + 6)[None, :] < k[:, None]
     rows = s[take]
     cols = np.repeat(np.arange(n), k)

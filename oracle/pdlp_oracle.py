@@ -133,16 +133,18 @@ def halpern_pdhg(lp, eps=1e-6, max_iter=100000, check_every=64, reflect=1.0, x0=
     cn, bn = np.linalg.norm(s.c), np.linalg.norm(s.b)
     omega = omega0 if omega0 is not None else (cn / bn if cn > 1e-10 and bn > 1e-10 else 1.0)
     eq = s.is_eq.astype(bool)
-    A32 = s.vals.astype(dtype)
+    # values and iterates are STORED in `dtype`; sums and updates are computed in FP64
+    A32 = s.vals.astype(dtype).astype(np.float64)
     rows = _rows(s)
 
     def Ax(v):
-        return np.bincount(rows, weights=A32 * v[s.colidx], minlength=s.m).astype(dtype)
+        return np.bincount(rows, weights=A32 * v.astype(np.float64)[s.colidx], minlength=s.m)
 
     def ATy(v):
-        return np.bincount(s.colidx, weights=A32 * v[rows], minlength=s.n).astype(dtype)
+        return np.bincount(s.colidx, weights=A32 * v.astype(np.float64)[rows], minlength=s.n)
 
-    c = s.c.astype(dtype); b = s.b.astype(dtype); l = s.lb.astype(dtype); u = s.ub.astype(dtype)
+    c = s.c.astype(dtype).astype(np.float64); b = s.b.astype(dtype).astype(np.float64)
+    l = s.lb.astype(dtype).astype(np.float64); u = s.ub.astype(dtype).astype(np.float64)
     x = (np.clip(np.zeros(s.n), s.lb, s.ub) if x0 is None else np.clip(x0 / dc, s.lb, s.ub)).astype(dtype)
     y = (np.zeros(s.m) if y0 is None else y0 / dr).astype(dtype)
     if y0 is not None:
@@ -156,17 +158,20 @@ def halpern_pdhg(lp, eps=1e-6, max_iter=100000, check_every=64, reflect=1.0, x0=
     info = {}
     while total < max_iter:
         tau, sigma = eta / omega, eta * omega
-        xt = np.clip(x - tau * (c + ATy(y)), l, u)
-        xh = 2 * xt - x
-        yt = y + sigma * (Ax(xh) - b)
-        yt = np.where(eq, yt, np.maximum(yt, 0)).astype(dtype)
+        x64, y64 = x.astype(np.float64), y.astype(np.float64)
+        xt = np.clip(x64 - tau * (c + ATy(y)), l, u)
+        xh = (2 * xt - x64).astype(dtype)
+        yt = y64 + sigma * (Ax(xh) - b)
+        yt = np.where(eq, yt, np.maximum(yt, 0))
         check = (k == 0) or ((total + 1) % check_every == 0)
         if check:
             r = np.sqrt(omega * np.sum((x - xt).astype(np.float64) ** 2) + np.sum((y - yt).astype(np.float64) ** 2) / omega)
         # Halpern step with reflection
         w = (k + 1.0) / (k + 2.0)
-        x = (w * ((1 + reflect) * xt - reflect * x) + (1 - w) * xa).astype(dtype)
-        y = (w * ((1 + reflect) * yt - reflect * y) + (1 - w) * ya).astype(dtype)
+        x = (w * ((1 + reflect) * xt - reflect * x64) + (1 - w) * xa.astype(np.float64)).astype(dtype)
+        y = (w * ((1 + reflect) * yt - reflect * y64) + (1 - w) * ya.astype(np.float64)).astype(dtype)
+        xt = xt.astype(dtype)
+        yt = yt.astype(dtype)
         k += 1
         total += 1
         if not check:

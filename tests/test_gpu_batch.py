@@ -1,0 +1,100 @@
+"""Batched engine on the GPU: many independent LPs in one persistent launch.
+
+Every instance's answer is checked by the oracle's FP64 KKT; objectives of the
+instances with committed HiGHS values are checked to 1e-6 relative."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import pdlp_oracle
+
+pytestmark = pytest.mark.gpu
+
+
+def upload_lps(ctx, lps):
+    stds = [lp.standard() for lp in lps]
+    mats = [(s.m, s.n, s.rowptr, s.colidx, s.vals) for s in stds]
+    ctx.batch_upload(mats, np.arange(len(stds), dtype=np.int32), np.concatenate([s.b for s in stds]),
+                     np.concatenate([s.c for s in stds]), np.concatenate([s.lb for s in stds]),
+                     np.concatenate([s.ub for s in stds]), np.concatenate([s.is_eq for s in stds]))
+    return stds
+
+
+def split(stds, x, y):
+    xo = np.cumsum([0] + [s.n for s in stds])
+    yo = np.cumsum([0] + [s.m for s in stds])
+    return [(x[xo[i]:xo[i + 1]], y[yo[i]:yo[i + 1]]) for i in range(len(stds))]
+
+
+@pytest.mark.parametrize("precision", ["fp32", "fp64"])
+def test_batch_uneven_all_optimal(ctx, golden, lpgen, precision):
+    lps = lpgen.uneven_batch(6, seed=12) + lpgen.uneven_batch(58, m_hi=600, seed=13)
+    stds = upload_lps(ctx, lps)
+    summ, per, x, y = ctx.batch_solve(precision=precision, eps=1e-6, max_iterations=100000)
+    assert np.all(per["status"] == 0), per["status"]
+    for i, (s, (xi, yi)) in enumerate(zip(stds, split(stds, x, y))):
+        k = pdlp_oracle.kkt(s, xi, yi)
+        assert k["rel_kkt"] <= 1.05e-6, (i, k)
+        assert abs(k["rel_kkt"] - per["rel_kkt"][i]) <= 1e-8 + 1e-3 * k["rel_kkt"]
+        if i < 6:
+            z = golden["highs"][f"batch12_{i}"]
+            assert abs(k["pobj"] - z) <= 1e-6 * max(1.0, abs(z)), (i, k["pobj"], z)
+
+
+def test_batch_matches_single_engine(ctx, lpgen):
+    lps = lpgen.uneven_batch(4, seed=31)
+    stds = upload_lps(ctx, lps)
+    _, per, x, y = ctx.batch_solve(precision="fp64", eps=1e-8, max_iterations=200000)
+    for s, (xi, yi) in zip(stds, split(stds, x, y)):
+        k = pdlp_oracle.kkt(s, xi, yi)
+        ctx.upload(s)
+        res, xs, ys = ctx.solve(engine="halpern", precision="fp64", eps=1e-8, max_iterations=200000)
+        assert res["status"] == "OPTIMAL"
+        assert abs(k["pobj"] - res["primal_objective"]) <= 1e-7 * max(1.0, abs(k["pobj"]))
+
+
+def test_batch_shared_matrix_family(ctx, golden, lpgen):
+    fam = lpgen.RefineryFamily()
+    p = np.vstack([fam.sample_params(1, 0), fam.sample_params(15, 77)])
+    inst = [fam.instance(q) for q in p]
+    stds = [lp.standard() for lp in inst]
+    s0 = stds[0]
+    ctx.batch_upload([(s0.m, s0.n, s0.rowptr, s0.colidx, s0.vals)], np.zeros(len(stds), np.int32),
+                     np.concatenate([s.b for s in stds]), np.concatenate([s.c for s in stds]),
+                     np.concatenate([s.lb for s in stds]), np.concatenate([s.ub for s in stds]),
+                     np.concatenate([s.is_eq for s in stds]))
+    _, per, x, y = ctx.batch_solve(precision="fp32", eps=1e-6, max_iterations=200000)
+    assert np.all(per["status"] == 0)
+    for i, (s, (xi, yi)) in enumerate(zip(stds, split(stds, x, y))):
+        k = pdlp_oracle.kkt(s, xi, yi)
+        assert k["rel_kkt"] <= 1.05e-6
+    z = golden["highs"]["refinery_p0"]
+    k0 = pdlp_oracle.kkt(stds[0], *split(stds, x, y)[0])
+    assert abs(k0["pobj"] - z) <= 1e-6 * abs(z)
+
+
+def test_batch_warm_start_and_weights(ctx, lpgen):
+    lps = lpgen.uneven_batch(8, m_hi=400, seed=40)
+    stds = upload_lps(ctx, lps)
+    _, per, x, y = ctx.batch_solve(precision="fp64", eps=1e-7)
+    cold = per["iterations"].copy()
+    _, per2, x2, y2 = ctx.batch_solve(x0=x, y0=y, precision="fp64", eps=1e-6)
+    assert np.all(per2["status"] == 0)
+    assert np.all(per2["iterations"] <= 128), (cold, per2["iterations"])
+
+
+def test_batch_iteration_limit(ctx, lpgen):
+    lps = lpgen.uneven_batch(5, m_hi=300, seed=41)
+    upload_lps(ctx, lps)
+    _, per, _, _ = ctx.batch_solve(precision="fp32", eps=1e-12, max_iterations=256)
+    assert np.all(per["status"] == 1) and np.all(per["iterations"] == 256)
+
+
+def test_batch_rejects_bad_input(ctx, b2p):
+    rp = np.array([0, 2], np.int32)
+    ci = np.array([1, 0], np.int32)  # not ascending
+    with pytest.raises(b2p.B2PError) as e:
+        ctx.batch_upload([(1, 2, rp, ci, np.ones(2))], np.zeros(1, np.int32), np.ones(1), np.ones(2), np.zeros(2),
+                         np.ones(2), np.zeros(1, np.uint8))
+    assert e.value.code == b2p.INVALID_ARGUMENT
