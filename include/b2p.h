@@ -165,6 +165,27 @@ int b2p_vector_op(void* ctx, int op, size_t n, double alpha, const double* a, co
 int b2p_dot(void* ctx, size_t n, const double* a, const double* b, double* out, b2p_timing_t* timing);
 int b2p_norm2(void* ctx, size_t n, const double* a, double* out, b2p_timing_t* timing);
 
+/* Allocation-free dot product.  No counterpart in the reference: it exists for
+ * callers that cannot let a library allocate device memory -- code recording a
+ * CUDA graph (cudaMalloc is not allowed while a stream is being captured) or an
+ * application that owns all device memory through its own pool.  The caller
+ * passes DEVICE pointers: a_dev, b_dev (n doubles each) and out_dev (1 double,
+ * receives a.b).  Work is queued on `stream` (a cudaStream_t; null = legacy
+ * default stream) and the call returns without synchronising.  No context is
+ * needed and nothing is allocated: the partial sums go to a fixed 32 KiB array
+ * in the library's device memory, which every GPU that loads the library keeps
+ * until the process exits.
+ *   - n may be at most B2P_DOT_NOALLOC_MAX_N; larger n returns B2P_TOO_LARGE
+ *     before anything is launched.
+ *   - The first call on a device looks the array's address up (set-up); make
+ *     that first call before any stream capture on that device.
+ *   - Every call shares the array (each call overwrites all it reads), so two
+ *     calls that can run at the same time on the GPU -- on different streams or
+ *     from different threads -- race; serialise them on one stream. */
+#define B2P_TOO_LARGE           8
+#define B2P_DOT_NOALLOC_MAX_N   8388608
+int b2p_dot_noalloc(const double* a_dev, const double* b_dev, size_t n, double* out_dev, void* stream);
+
 /* ---- single LP ----
  * Standard form (src/first_order_solver.cpp:68-101): minimise c.x subject to
  * (A x)_i <= b_i where is_eq[i] == 0, (A x)_i == b_i where is_eq[i] == 1, and

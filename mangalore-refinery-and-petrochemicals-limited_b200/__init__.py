@@ -18,11 +18,12 @@ from . import lpgen  # noqa: F401  (workload generators)
 _HERE = Path(__file__).resolve().parent
 LIB_PATH = Path(os.environ.get("B2P_LIB", _HERE / "libb2p.so"))
 
-OK, GPU_UNAVAILABLE, GPU_UNINITIALIZED, OUT_OF_MEMORY, INVALID_ARGUMENT, EXECUTION_FAILED, NO_LP, TIMEOUT = range(8)
+OK, GPU_UNAVAILABLE, GPU_UNINITIALIZED, OUT_OF_MEMORY, INVALID_ARGUMENT, EXECUTION_FAILED, NO_LP, TIMEOUT, TOO_LARGE = range(9)
+DOT_NOALLOC_MAX_N = 8388608
 STATUS_NAMES = ["OPTIMAL", "MAX_ITERATIONS", "NUMERICAL_FAILURE", "INFEASIBLE_DETECTED", "UNBOUNDED_DETECTED",
                 "INTERRUPTED"]
 CALL_NAMES = ["OK", "GPU_UNAVAILABLE", "GPU_UNINITIALIZED", "OUT_OF_MEMORY", "INVALID_ARGUMENT", "EXECUTION_FAILED",
-              "NO_LP", "TIMEOUT"]
+              "NO_LP", "TIMEOUT", "TOO_LARGE"]
 ENGINES = {"reference": 0, "halpern": 1}
 PRECISIONS = {"fp64": 0, "fp32": 1}
 
@@ -84,6 +85,7 @@ SIGNATURES = {
     "b2p_vector_op": (C.c_int, [_P, C.c_int, C.c_size_t, C.c_double, _F64P, _P, _F64P, C.POINTER(Timing)]),
     "b2p_dot": (C.c_int, [_P, C.c_size_t, _F64P, _F64P, C.POINTER(C.c_double), C.POINTER(Timing)]),
     "b2p_norm2": (C.c_int, [_P, C.c_size_t, _F64P, C.POINTER(C.c_double), C.POINTER(Timing)]),
+    "b2p_dot_noalloc": (C.c_int, [_P, _P, C.c_size_t, _P, _P]),
     "b2p_upload_lp": (C.c_int, [_P, C.c_int, C.c_int, C.c_int64, _I32P, _I32P, _F64P, _F64P, _F64P, _F64P, _F64P,
                                 _U8P]),
     "b2p_solve": (C.c_int, [_P, C.POINTER(Params), _P, _P, C.POINTER(Result), _P, _P]),
