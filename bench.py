@@ -49,7 +49,26 @@ def parse():
     ap.add_argument("--eps", type=float, default=1e-6)
     ap.add_argument("--no-fp64", action="store_true", help="skip the plain FP64 comparison leg")
     ap.add_argument("--cpu-sample-iters", type=int, default=20)
+    ap.add_argument("--profile", action="store_true",
+                    help="profiling case: one short solve, then the two iteration kernels once each inside the "
+                         "NVTX range 'kernel_timing' (for ncu --nvtx-include kernel_timing/)")
     return ap.parse_args()
+
+
+def profile_case(args):
+    import torch
+    torch.cuda.set_device(0)
+    torch.cuda.set_stream(torch.cuda.Stream())
+    b2p, lp, _ = make_lp(args.workload)
+    with b2p.Context(0) as ctx:
+        ctx.set_stream(torch.cuda.current_stream().cuda_stream)
+        ctx.upload(lp.standard())
+        for prec in ("fp32", "fp64"):
+            ctx.solve(engine="halpern", precision=prec, eps=args.eps, max_iterations=256)
+            torch.cuda.nvtx.range_push("kernel_timing")
+            kt = ctx.kernel_timing(reps=1, engine="halpern", precision=prec, eps=args.eps)
+            torch.cuda.nvtx.range_pop()
+            print(json.dumps({"precision": prec, **kt}), flush=True)
 
 
 def make_lp(workload):
@@ -239,6 +258,9 @@ def run_reference(args):
 
 def main():
     args = parse()
+    if args.profile:
+        profile_case(args)
+        return
     if args.impl == "reference":
         run_reference(args)
         return

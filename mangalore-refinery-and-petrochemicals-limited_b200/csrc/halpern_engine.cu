@@ -69,7 +69,7 @@ struct HalpernWork {
     // autotuned launch shape (lanes per row L, rows per lane group R) of the two
     // iteration kernels, keyed by the LP's shape and precision
     long long tuned_key = -1;
-    int Lc = 8, Rc = 1, Lr = 8, Rr = 1;
+    int Lc = 8, Rc = 1, Lr = 8, Rr = 1, Tc = 256, Tr = 256;
     Ctrl* host_ctrl = nullptr;     // pinned, 2 slots
     cudaEvent_t ev[2] = {nullptr, nullptr};
     ~HalpernWork() {
@@ -89,7 +89,7 @@ namespace {
 constexpr int TB = 256;
 
 __device__ __forceinline__ double block_sum_to(double v, double* slot) {
-    __shared__ double sh[TB / 32];
+    __shared__ double sh[32];  // one slot per warp of a CTA of up to 1024 threads
     v = warp_sum(v);
     int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     if (lane == 0) sh[w] = v;
@@ -280,10 +280,13 @@ __device__ __forceinline__ int ld_stream(const int* p, unsigned long long pol) {
 // the first L entries of the R rows, then their R gathers -- is issued before any
 // is consumed, so each warp keeps several independent memory requests in flight
 // (the kernel is bound by memory latency x parallelism, not by arithmetic).
+// Each CTA owns one contiguous range of rows, so its warps gather from the same
+// neighbourhood of the operand vector (for structured LPs such as block-angular
+// ones, one block's slice stays in L1); the CTA size is part of the tuned shape.
 // All 32 lanes of a warp stay converged through the shuffles.  Sums and updates
 // are FP64; VT only sets the bytes streamed for values and xh.
 template <typename VT, typename GT, int L, int R, int MODE, bool PRIMAL>
-__global__ void __launch_bounds__(TB) k_iter(IterArgs<VT, GT> a, int it) {
+__global__ void __launch_bounds__(1024) k_iter(IterArgs<VT, GT> a, int it) {
     const Ctrl* ctrl = a.ctrl;
     if (ctrl->done) return;
     const unsigned long long pol = evict_first_policy();
@@ -296,22 +299,26 @@ __global__ void __launch_bounds__(TB) k_iter(IterArgs<VT, GT> a, int it) {
     const int sub = lane & (L - 1);
     const int rpw = 32 / L;
     const int span = rpw * R;
-    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int nwarps = (gridDim.x * blockDim.x) >> 5;
+    const int wpc = blockDim.x >> 5;
+    const int warp_in_cta = threadIdx.x >> 5;
+    // this CTA's rows: [row0, row1), a multiple of span per CTA
+    const long long per_cta = (((long long)a.rows + gridDim.x - 1) / gridDim.x + span - 1) / span * span;
+    const int row0 = (int)min((long long)a.rows, (long long)blockIdx.x * per_cta);
+    const int row1 = (int)min((long long)a.rows, (long long)row0 + per_cta);
     double acc_r = 0.0, acc_d = 0.0;
-    for (int base = warp * span; base < a.rows; base += nwarps * span) {
+    for (int base = row0 + warp_in_cta * span; base < row1; base += wpc * span) {
         int r[R], k0[R], k1[R];
 #pragma unroll
         for (int u = 0; u < R; ++u) {
             r[u] = base + u * rpw + lane / L;
-            const bool v = r[u] < a.rows;
+            const bool v = r[u] < row1;
             k0[u] = v ? ld_stream(a.ptr + r[u], pol) : 0;
             k1[u] = v ? ld_stream(a.ptr + r[u] + 1, pol) : 0;
         }
         double zr[R], cst[R];
 #pragma unroll
         for (int u = 0; u < R; ++u) {
-            const bool lead = sub == 0 && r[u] < a.rows;
+            const bool lead = sub == 0 && r[u] < row1;
             zr[u] = lead ? a.z[r[u]] : 0.0;
             cst[u] = lead ? a.cost[r[u]] : 0.0;
         }
@@ -338,7 +345,7 @@ __global__ void __launch_bounds__(TB) k_iter(IterArgs<VT, GT> a, int it) {
         }
 #pragma unroll
         for (int u = 0; u < R; ++u) {
-            if (sub != 0 || r[u] >= a.rows) continue;
+            if (sub != 0 || r[u] >= row1) continue;
             const int row = r[u];
             double zt;
             if (PRIMAL) {
@@ -522,24 +529,24 @@ int pick_lanes(double mean_len, int requested) {
 }
 
 template <typename VT, typename GT, int R, int MODE, bool PRIMAL>
-void launch_iter_LR(int L, unsigned grid, cudaStream_t s, const IterArgs<VT, GT>& a, int it) {
+void launch_iter_LR(int L, unsigned grid, int tb, cudaStream_t s, const IterArgs<VT, GT>& a, int it) {
     switch (L) {
-        case 2: k_iter<VT, GT, 2, R, MODE, PRIMAL><<<grid, TB, 0, s>>>(a, it); break;
-        case 4: k_iter<VT, GT, 4, R, MODE, PRIMAL><<<grid, TB, 0, s>>>(a, it); break;
-        case 8: k_iter<VT, GT, 8, R, MODE, PRIMAL><<<grid, TB, 0, s>>>(a, it); break;
-        case 16: k_iter<VT, GT, 16, R, MODE, PRIMAL><<<grid, TB, 0, s>>>(a, it); break;
-        default: k_iter<VT, GT, 32, R, MODE, PRIMAL><<<grid, TB, 0, s>>>(a, it); break;
+        case 2: k_iter<VT, GT, 2, R, MODE, PRIMAL><<<grid, tb, 0, s>>>(a, it); break;
+        case 4: k_iter<VT, GT, 4, R, MODE, PRIMAL><<<grid, tb, 0, s>>>(a, it); break;
+        case 8: k_iter<VT, GT, 8, R, MODE, PRIMAL><<<grid, tb, 0, s>>>(a, it); break;
+        case 16: k_iter<VT, GT, 16, R, MODE, PRIMAL><<<grid, tb, 0, s>>>(a, it); break;
+        default: k_iter<VT, GT, 32, R, MODE, PRIMAL><<<grid, tb, 0, s>>>(a, it); break;
     }
 }
 
 // Plain iterations use R rows per lane group; the two reduction iterations of a chunk use R = 1.
 template <typename VT, typename GT, bool PRIMAL>
-void launch_iter(int mode, int L, int R, unsigned grid, cudaStream_t s, const IterArgs<VT, GT>& a, int it) {
-    if (mode == M_FIRST) launch_iter_LR<VT, GT, 1, M_FIRST, PRIMAL>(L, grid, s, a, it);
-    else if (mode == M_CHECK) launch_iter_LR<VT, GT, 1, M_CHECK, PRIMAL>(L, grid, s, a, it);
-    else if (R >= 4) launch_iter_LR<VT, GT, 4, M_PLAIN, PRIMAL>(L, grid, s, a, it);
-    else if (R == 2) launch_iter_LR<VT, GT, 2, M_PLAIN, PRIMAL>(L, grid, s, a, it);
-    else launch_iter_LR<VT, GT, 1, M_PLAIN, PRIMAL>(L, grid, s, a, it);
+void launch_iter(int mode, int L, int R, unsigned grid, int tb, cudaStream_t s, const IterArgs<VT, GT>& a, int it) {
+    if (mode == M_FIRST) launch_iter_LR<VT, GT, 1, M_FIRST, PRIMAL>(L, grid, tb, s, a, it);
+    else if (mode == M_CHECK) launch_iter_LR<VT, GT, 1, M_CHECK, PRIMAL>(L, grid, tb, s, a, it);
+    else if (R >= 4) launch_iter_LR<VT, GT, 4, M_PLAIN, PRIMAL>(L, grid, tb, s, a, it);
+    else if (R == 2) launch_iter_LR<VT, GT, 2, M_PLAIN, PRIMAL>(L, grid, tb, s, a, it);
+    else launch_iter_LR<VT, GT, 1, M_PLAIN, PRIMAL>(L, grid, tb, s, a, it);
 }
 
 void launch_kkt(int Lr, int Lc, unsigned gr, unsigned gc, cudaStream_t s, const DevLP& lp, HalpernWork* w, Ctrl* ctrl) {
@@ -638,14 +645,15 @@ struct Ops<float> {
     static float* xh(HalpernWork* w) { return w->xh32.p; }
 };
 
-inline unsigned iter_grid(int64_t rows, int L, int R, int sm_count) {
-    return grid_for((rows * L + R - 1) / R, TB, sm_count, 8);
+// One resident wave: 2048 / tb CTAs per SM, each owning a contiguous row range.
+inline unsigned iter_grid(int64_t rows, int L, int R, int tb, int sm_count) {
+    return grid_for((rows * L + R - 1) / R, tb, sm_count, 2048 / tb);
 }
 
-// Times candidate (L, R) launch shapes of the primal and dual kernels on the
-// uploaded LP (plain iterations from the current iterates, CUDA events on the
-// context stream) and keeps the fastest of each.  The caller re-initialises the
-// iterates afterwards.  Explicit lanes_per_row skips the search.
+// Times candidate (L, R, CTA size) launch shapes of the primal and dual kernels
+// on the uploaded LP (plain iterations from the current iterates, CUDA events on
+// the context stream) and keeps the fastest of each.  The caller re-initialises
+// the iterates afterwards.  Explicit lanes_per_row skips the search.
 template <typename MT>
 int autotune_shapes(Ctx* ctx, HalpernWork* w, const b2p_params* p) {
     DevLP& L = ctx->lp;
@@ -653,6 +661,7 @@ int autotune_shapes(Ctx* ctx, HalpernWork* w, const b2p_params* p) {
     if (p->lanes_per_row > 0) {
         w->Lc = w->Lr = pick_lanes(0, p->lanes_per_row);
         w->Rc = w->Rr = 1;
+        w->Tc = w->Tr = 256;
         w->tuned_key = -1;
         return B2P_OK;
     }
@@ -672,17 +681,17 @@ int autotune_shapes(Ctx* ctx, HalpernWork* w, const b2p_params* p) {
         const double mean = primal ? L.mean_col_len : L.mean_row_len;
         const int base_L = pick_lanes(mean, 0);
         float best = 1e30f;
-        int bestL = base_L, bestR = 1;
+        int bestL = base_L, bestR = 1, bestT = 256;
         for (int Lc : {base_L / 2, base_L, base_L * 2}) {
             if (Lc < 2 || Lc > 32) continue;
-            for (int R : {1, 2, 4}) {
+            for (int R : {1, 2, 4}) for (int tb : {256, 512, 1024}) {
                 const int64_t rows = primal ? n : m;
-                unsigned g = iter_grid(rows, Lc, R, ctx->sm_count);
+                unsigned g = iter_grid(rows, Lc, R, tb, ctx->sm_count);
                 float tot = 0.f;
                 for (int rep = 0; rep < 4; ++rep) {
                     cudaEventRecord(e0, s);
-                    if (primal) launch_iter<MT, double, true>(M_PLAIN, Lc, R, g, s, pa, rep);
-                    else launch_iter<MT, MT, false>(M_PLAIN, Lc, R, g, s, da, rep);
+                    if (primal) launch_iter<MT, double, true>(M_PLAIN, Lc, R, g, tb, s, pa, rep);
+                    else launch_iter<MT, MT, false>(M_PLAIN, Lc, R, g, tb, s, da, rep);
                     cudaEventRecord(e1, s);
                     B2P_LAUNCH(ctx);
                     B2P_CUDA(ctx, cudaEventSynchronize(e1));
@@ -695,11 +704,12 @@ int autotune_shapes(Ctx* ctx, HalpernWork* w, const b2p_params* p) {
                     best = tot;
                     bestL = Lc;
                     bestR = R;
+                    bestT = tb;
                 }
             }
         }
-        if (primal) { w->Lc = bestL; w->Rc = bestR; }
-        else { w->Lr = bestL; w->Rr = bestR; }
+        if (primal) { w->Lc = bestL; w->Rc = bestR; w->Tc = bestT; }
+        else { w->Lr = bestL; w->Rr = bestR; w->Tr = bestT; }
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
@@ -712,10 +722,11 @@ int run_chunks(Ctx* ctx, HalpernWork* w, const b2p_params* p, double time_limit_
     DevLP& L = ctx->lp;
     cudaStream_t s = ctx->stream;
     const int m = L.m, n = L.n, K = p->check_every;
-    const int Lr = w->Lr, Lc = w->Lc, Rr = w->Rr, Rc = w->Rc;
-    // R = 1 grids serve the reduction iterations and the KKT kernels
-    unsigned gr = iter_grid(m, Lr, 1, ctx->sm_count), gc = iter_grid(n, Lc, 1, ctx->sm_count);
-    unsigned grR = iter_grid(m, Lr, Rr, ctx->sm_count), gcR = iter_grid(n, Lc, Rc, ctx->sm_count);
+    const int Lr = w->Lr, Lc = w->Lc, Rr = w->Rr, Rc = w->Rc, Tr = w->Tr, Tc = w->Tc;
+    // R = 1 grids serve the two reduction iterations; the KKT kernels use 256-thread grids
+    unsigned gr = iter_grid(m, Lr, 1, Tr, ctx->sm_count), gc = iter_grid(n, Lc, 1, Tc, ctx->sm_count);
+    unsigned grR = iter_grid(m, Lr, Rr, Tr, ctx->sm_count), gcR = iter_grid(n, Lc, Rc, Tc, ctx->sm_count);
+    unsigned gkr = iter_grid(m, Lr, 1, TB, ctx->sm_count), gkc = iter_grid(n, Lc, 1, TB, ctx->sm_count);
     Ctrl* ctrl = w->ctrl.p;
     IterArgs<MT, double> pa{L.t_rowptr.p, L.t_colidx.p, Ops<MT>::stv(w), w->y.p, w->c64.p, w->l64.p, w->u64.p,
                             nullptr, w->x.p, Ops<MT>::xh(w), w->xa.p, w->xt.p, ctrl, n, p->reflection};
@@ -725,14 +736,14 @@ int run_chunks(Ctx* ctx, HalpernWork* w, const b2p_params* p, double time_limit_
         for (int i = 0; i < K; ++i) {
             int mode = (i == 0) ? M_FIRST : (i == K - 1 ? M_CHECK : M_PLAIN);
             if (mode == M_PLAIN) {
-                launch_iter<MT, double, true>(mode, Lc, Rc, gcR, s, pa, i);
-                launch_iter<MT, MT, false>(mode, Lr, Rr, grR, s, da, i);
+                launch_iter<MT, double, true>(mode, Lc, Rc, gcR, Tc, s, pa, i);
+                launch_iter<MT, MT, false>(mode, Lr, Rr, grR, Tr, s, da, i);
             } else {
-                launch_iter<MT, double, true>(mode, Lc, 1, gc, s, pa, i);
-                launch_iter<MT, MT, false>(mode, Lr, 1, gr, s, da, i);
+                launch_iter<MT, double, true>(mode, Lc, 1, gc, Tc, s, pa, i);
+                launch_iter<MT, MT, false>(mode, Lr, 1, gr, Tr, s, da, i);
             }
         }
-        launch_kkt(Lr, Lc, gr, gc, s, L, w, ctrl);
+        launch_kkt(Lr, Lc, gkr, gkc, s, L, w, ctrl);
         k_control<<<1, 1, 0, s>>>(ctrl);
         k_restart<<<grid_for(std::max(m, n), TB, ctx->sm_count, 8), TB, 0, s>>>(m, n, ctrl, w->x.p, w->xa.p, w->xt.p,
                                                                                w->y.p, w->ya.p, w->yt.p, nullptr);
@@ -911,8 +922,8 @@ int kernel_timing_T(Ctx* ctx, HalpernWork* w, const b2p_params* p, int reps, dou
     DevLP& L = ctx->lp;
     cudaStream_t s = ctx->stream;
     const int m = L.m, n = L.n;
-    const int Lr = w->Lr, Lc = w->Lc, Rr = w->Rr, Rc = w->Rc;
-    unsigned gr = iter_grid(m, Lr, Rr, ctx->sm_count), gc = iter_grid(n, Lc, Rc, ctx->sm_count);
+    const int Lr = w->Lr, Lc = w->Lc, Rr = w->Rr, Rc = w->Rc, Tr = w->Tr, Tc = w->Tc;
+    unsigned gr = iter_grid(m, Lr, Rr, Tr, ctx->sm_count), gc = iter_grid(n, Lc, Rc, Tc, ctx->sm_count);
     Ctrl* ctrl = w->ctrl.p;
     // re-open the (finished) control block for plain iterations, restore it afterwards
     Ctrl saved;
@@ -930,9 +941,9 @@ int kernel_timing_T(Ctx* ctx, HalpernWork* w, const b2p_params* p, int reps, dou
     double tp = 0, td = 0;
     for (int r = 0; r < reps; ++r) {
         cudaEventRecord(e[0], s);
-        launch_iter<MT, double, true>(M_PLAIN, Lc, Rc, gc, s, pa, r);
+        launch_iter<MT, double, true>(M_PLAIN, Lc, Rc, gc, Tc, s, pa, r);
         cudaEventRecord(e[1], s);
-        launch_iter<MT, MT, false>(M_PLAIN, Lr, Rr, gr, s, da, r);
+        launch_iter<MT, MT, false>(M_PLAIN, Lr, Rr, gr, Tr, s, da, r);
         cudaEventRecord(e[2], s);
         B2P_LAUNCH(ctx);
         B2P_CUDA(ctx, cudaEventSynchronize(e[2]));
