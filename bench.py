@@ -339,15 +339,22 @@ def main():
     barrier(world)
     torch.cuda.synchronize()
     e0.record(stream)
+    up_s = solve_s = 0.0
     for _ in range(args.steps):
+        t0 = time.perf_counter()
         ctx.upload(plp)
+        t1 = time.perf_counter()
         res, x, y = ctx.solve(precision="fp32", **common)
+        t2 = time.perf_counter()
+        up_s += t1 - t0
+        solve_s += t2 - t1
     e1.record(stream)
     torch.cuda.synchronize()
     barrier(world)
     e2e_ms = max_over_ranks(e0.elapsed_time(e1), world)
     e2e = {"value": (args.steps * world) / (e2e_ms / 1e3), "unit": "LPs/s", "h2d_bytes_per_step": h2d,
-           "d2h_bytes_per_step": d2h}
+           "d2h_bytes_per_step": d2h, "upload_ms_per_step": 1e3 * up_s / args.steps,
+           "solve_ms_per_step": 1e3 * solve_s / args.steps, "iterations": res["iterations"]}
     cpu = None
     if rank == 0 and world == 1:
         cpu = cpu_reference_sample(lp, args.cpu_sample_iters, fp64["iterations"] if fp64 else iters)

@@ -110,8 +110,10 @@ typedef struct {
     double  restart_artificial;     /* 0.36 */
     double  primal_weight;          /* 0 = ||c||/||b|| of the scaled LP */
     double  step_safety;            /* 0.998 / ||A||_2 */
-    int     refinement_rounds;      /* FP64 iterative-refinement rounds after the FP32 solve (0 = off) */
-    double  refinement_eps;         /* target rel KKT of the refined answer */
+    int     refinement_rounds;      /* FP64 iterative refinement: at each restart the LP is re-centred on the
+                                       current point with residuals b - A x, c + A^T y computed from the
+                                       FP64 matrix.  -1 = on for FP32 / off for FP64 (default), 0 = off,
+                                       > 0 = on */
     double  time_limit_s;           /* 0 = none */
     int     lanes_per_row;          /* 0 = auto; else 1,2,4,8,16,32 lanes per CSR row */
 } b2p_params;

@@ -47,7 +47,7 @@ class Params(C.Structure):
                 ("eps_rel_kkt", C.c_double), ("check_every", C.c_int), ("ruiz_iterations", C.c_int),
                 ("reflection", C.c_double), ("restart_sufficient", C.c_double), ("restart_necessary", C.c_double),
                 ("restart_artificial", C.c_double), ("primal_weight", C.c_double), ("step_safety", C.c_double),
-                ("refinement_rounds", C.c_int), ("refinement_eps", C.c_double), ("time_limit_s", C.c_double),
+                ("refinement_rounds", C.c_int), ("time_limit_s", C.c_double),
                 ("lanes_per_row", C.c_int)]
 
 

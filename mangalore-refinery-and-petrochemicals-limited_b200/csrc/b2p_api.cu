@@ -230,8 +230,7 @@ void b2p_params_default(b2p_params* p) {
     p->restart_artificial = 0.36;
     p->primal_weight = 0.0;
     p->step_safety = 0.998;
-    p->refinement_rounds = 0;
-    p->refinement_eps = 1e-8;
+    p->refinement_rounds = -1;
     p->time_limit_s = 0.0;
     p->lanes_per_row = 0;
 }

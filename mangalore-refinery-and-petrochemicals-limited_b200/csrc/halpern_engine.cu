@@ -51,10 +51,17 @@ struct Ctrl {
     double r0, rprev;
     double rel_p, rel_d, rel_g, pobj, dobj;
     double eps, beta_s, beta_n, beta_a, bnorm, cnorm;
+    // refinement: the solved (correction) problem maps back to the original LP as
+    // x = xbar + pscale * dc * xt, y = ybar + dscale * dr * yt; the solve also stops
+    // (status kInnerDone) once its fixed-point residual fell to inner_tol * r_first
+    double pscale, dscale, inner_tol, r_first;
     long long k_base, total, max_iter, restarts;
     int K;
     int done, status, restart, first_after_restart;
 };
+
+// private status of a solve that reached its inner tolerance (refinement continues)
+constexpr int kInnerDone = 100;
 
 struct HalpernWork {
     int m = -1, n = -1;
@@ -65,6 +72,9 @@ struct HalpernWork {
     DBuf<double> x, xa, xt, y, ya, yt;  // FP64 iterates (both precisions)
     DBuf<double> xh64;                   // gathered operand, FP64 engine
     DBuf<float> xh32, yg32;              // gathered operands, mixed engine
+    // FP64 re-centring: current centre in the original space, A xbar, A^T ybar, shifted dual bound
+    bool recenter = false;
+    DBuf<double> xbar, ybar, axbar, atybar, ylb_s;
     DBuf<Ctrl> ctrl;
     // autotuned launch shape (lanes per row L, rows per lane group R) of the two
     // iteration kernels, keyed by the LP's shape and precision
@@ -211,8 +221,8 @@ __global__ void k_pow_init(int n, double* __restrict__ v) {
 __global__ void k_init_iterates(int m, int n, const double* __restrict__ l, const double* __restrict__ u,
                                 const double* __restrict__ x0, const double* __restrict__ y0,
                                 const double* __restrict__ dr, const double* __restrict__ dc,
-                                const uint8_t* __restrict__ is_eq, double* x, double* xa, double* xt, double* y,
-                                double* ya, double* yt, float* yg32) {
+                                const uint8_t* __restrict__ is_eq, const double* __restrict__ ylb, double* x,
+                                double* xa, double* xt, double* y, double* ya, double* yt, float* yg32) {
     int tid = blockIdx.x * blockDim.x + threadIdx.x, st = gridDim.x * blockDim.x;
     for (int j = tid; j < n; j += st) {
         double v = x0 ? x0[j] / dc[j] : 0.0;
@@ -221,7 +231,8 @@ __global__ void k_init_iterates(int m, int n, const double* __restrict__ l, cons
     }
     for (int i = tid; i < m; i += st) {
         double v = y0 ? y0[i] / dr[i] : 0.0;
-        if (!is_eq[i] && v < 0.0) v = 0.0;
+        const double lbv = ylb ? ylb[i] : 0.0;
+        if (!is_eq[i] && v < lbv) v = lbv;
         y[i] = v; ya[i] = v; yt[i] = v;
         if (yg32) yg32[i] = (float)v;
     }
@@ -242,6 +253,7 @@ struct IterArgs {
     const double* lo;      // l (primal)
     const double* hi;      // u (primal)
     const uint8_t* is_eq;  // dual
+    const double* ylb;     // dual: lower bound of y on <= rows in scaled space (null = 0; refinement shifts it)
     double* z;             // x or y, updated in place
     VT* zh;                // primal: xh out (dual: unused)
     const double* za;      // anchor
@@ -353,7 +365,10 @@ __global__ void __launch_bounds__(1024) k_iter(IterArgs<VT, GT> a, int it) {
                 a.zh[row] = (VT)(2.0 * zt - zr[u]);
             } else {
                 zt = zr[u] + step * (s[u] - cst[u]);
-                if (!a.is_eq[row] && zt < 0.0) zt = 0.0;
+                if (!a.is_eq[row]) {
+                    const double lbv = a.ylb ? a.ylb[row] : 0.0;
+                    if (zt < lbv) zt = lbv;
+                }
             }
             const double za = a.za[row];
             a.z[row] = wk * ((1.0 + rho) * zt - rho * zr[u]) + wa * za;
@@ -377,13 +392,25 @@ __global__ void __launch_bounds__(1024) k_iter(IterArgs<VT, GT> a, int it) {
 
 // ------------------------------------------------------------------ FP64 KKT of T(z) on the original LP
 // rows: primal residual of x = dc*xt and the b.y term of y = dr*yt
+// Point of the ORIGINAL LP that the solved problem's T(z) stands for:
+//   x = xbar + pscale * dc * xt,  y = ybar + dscale * dr * yt
+// (xbar = ybar = null, pscale = dscale = 1 outside refinement).  A x and A^T y of
+// that point use the precomputed A xbar / A^T ybar.
+struct KktMap {
+    const double* xbar;   // n
+    const double* ybar;   // m
+    const double* axbar;  // m: A xbar
+    const double* atybar; // n: A^T ybar
+};
+
 template <int L>
 __global__ void __launch_bounds__(TB) k_kkt_rows(int m, const int32_t* __restrict__ ptr, const int32_t* __restrict__ idx,
                                                  const double* __restrict__ v64, const double* __restrict__ xt,
                                                  const double* __restrict__ yt, const double* __restrict__ b,
                                                  const uint8_t* __restrict__ is_eq, const double* __restrict__ dr,
-                                                 Ctrl* ctrl) {
+                                                 KktMap map, Ctrl* ctrl) {
     if (ctrl->done) return;
+    const double ps = ctrl->pscale, ds = ctrl->dscale;
     const int lane = threadIdx.x & 31, sub = lane & (L - 1), rpw = 32 / L;
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
     double p2 = 0.0, by = 0.0;
@@ -396,11 +423,11 @@ __global__ void __launch_bounds__(TB) k_kkt_rows(int m, const int32_t* __restric
 #pragma unroll
         for (int o = L / 2; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
         if (valid && sub == 0) {
-            double ax = s / dr[r];
+            double ax = (map.axbar ? map.axbar[r] : 0.0) + ps * (s / dr[r]);
             double rp = ax - b[r];
             if (!is_eq[r]) rp = fmax(rp, 0.0);
             p2 += rp * rp;
-            by += b[r] * (dr[r] * yt[r]);
+            by += b[r] * ((map.ybar ? map.ybar[r] : 0.0) + ds * (dr[r] * yt[r]));
         }
     }
     block_sum_to(p2, &ctrl->acc[A_PRES2]);
@@ -413,8 +440,9 @@ __global__ void __launch_bounds__(TB) k_kkt_cols(int n, const int32_t* __restric
                                                  const double* __restrict__ v64, const double* __restrict__ yt,
                                                  const double* __restrict__ xt, const double* __restrict__ c,
                                                  const double* __restrict__ lb, const double* __restrict__ ub,
-                                                 const double* __restrict__ dc, Ctrl* ctrl) {
+                                                 const double* __restrict__ dc, KktMap map, Ctrl* ctrl) {
     if (ctrl->done) return;
+    const double ps = ctrl->pscale, ds = ctrl->dscale;
     const int lane = threadIdx.x & 31, sub = lane & (L - 1), rpw = 32 / L;
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
     double d2 = 0.0, pc = 0.0, lam_t = 0.0;
@@ -427,12 +455,12 @@ __global__ void __launch_bounds__(TB) k_kkt_cols(int n, const int32_t* __restric
 #pragma unroll
         for (int o = L / 2; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
         if (valid && sub == 0) {
-            double g = c[j] + s / dc[j];
+            double g = c[j] + (map.atybar ? map.atybar[j] : 0.0) + ds * (s / dc[j]);
             bool fl = isfinite(lb[j]), fu = isfinite(ub[j]);
             double lam = (fl && fu) ? g : (fl ? fmax(g, 0.0) : (fu ? fmin(g, 0.0) : 0.0));
             double rd = g - lam;
             d2 += rd * rd;
-            double x = dc[j] * xt[j];
+            double x = (map.xbar ? map.xbar[j] : 0.0) + ps * (dc[j] * xt[j]);
             pc += c[j] * x;
             if (lam > 0.0) lam_t += lam * lb[j];
             else if (lam < 0.0) lam_t += lam * ub[j];
@@ -452,6 +480,7 @@ __global__ void k_control(Ctrl* c) {
     if (c->first_after_restart) {
         c->r0 = sqrt(om * a[A_RX2_FIRST] + a[A_RY2_FIRST] / om);
         c->rprev = c->r0;
+        if (c->r_first <= 0.0) c->r_first = c->r0;  // residual of the starting point of this solve
     }
     c->total += c->K;
     double pres = sqrt(a[A_PRES2]), dres = sqrt(a[A_DRES2]);
@@ -471,6 +500,9 @@ __global__ void k_control(Ctrl* c) {
     } else if (c->total >= c->max_iter) {
         c->done = 1;
         c->status = B2P_STATUS_MAX_ITERATIONS;
+    } else if (c->inner_tol > 0.0 && r <= c->inner_tol * c->r_first) {
+        c->done = 1;
+        c->status = kInnerDone;
     }
     c->restart = 0;
     c->first_after_restart = 0;
@@ -511,13 +543,69 @@ __global__ void k_restart(int m, int n, const Ctrl* __restrict__ c, double* x, d
     }
 }
 
-// unscale T(z) into FP64 outputs: x = dc * xt, y = dr * yt
+// unscale T(z) into FP64 outputs of the original LP: x = xbar + dc * xt, y = ybar + dr * yt
 __global__ void k_unscale(int m, int n, const double* __restrict__ xt, const double* __restrict__ yt,
-                          const double* __restrict__ dr, const double* __restrict__ dc, double* __restrict__ xo,
-                          double* __restrict__ yo) {
+                          const double* __restrict__ dr, const double* __restrict__ dc, const double* __restrict__ xbar,
+                          const double* __restrict__ ybar, double* __restrict__ xo, double* __restrict__ yo) {
     int tid = blockIdx.x * blockDim.x + threadIdx.x, st = gridDim.x * blockDim.x;
-    for (int j = tid; j < n; j += st) xo[j] = dc[j] * xt[j];
-    for (int i = tid; i < m; i += st) yo[i] = dr[i] * yt[i];
+    for (int j = tid; j < n; j += st) xo[j] = (xbar ? xbar[j] : 0.0) + dc[j] * xt[j];
+    for (int i = tid; i < m; i += st) yo[i] = (ybar ? ybar[i] : 0.0) + dr[i] * yt[i];
+}
+
+// ------------------------------------------------------------------ FP64 re-centring (iterative refinement)
+// At a restart the Halpern iterate and anchor become T(z).  With re-centring on,
+// the problem is instead rewritten around that point (xbar, ybar) in the original
+// space -- an exact change of variables, so PDHG proceeds unchanged:
+//   b' = b - A xbar,  c' = c + A^T ybar,  l' = l - xbar,  u' = u - xbar,
+//   y' >= -ybar on <= rows,   and the iterates restart at 0.
+// A xbar and A^T ybar use the FP64 original matrix, so the FP32 matrix values
+// and xh only ever act on the (small) correction: the residual is exact to FP64
+// after every restart.  The three kernels return at once unless the control
+// kernel has just decided to restart.
+__global__ void k_rc_update(int m, int n, const Ctrl* __restrict__ c, const double* __restrict__ dr,
+                            const double* __restrict__ dc, double* xbar, double* ybar, double* x, double* xa,
+                            double* xt, double* y, double* ya, double* yt) {
+    if (c->done || !c->restart) return;
+    int tid = blockIdx.x * blockDim.x + threadIdx.x, st = gridDim.x * blockDim.x;
+    for (int j = tid; j < n; j += st) {
+        xbar[j] += dc[j] * xt[j];
+        x[j] = 0.0; xa[j] = 0.0; xt[j] = 0.0;
+    }
+    for (int i = tid; i < m; i += st) {
+        ybar[i] += dr[i] * yt[i];
+        y[i] = 0.0; ya[i] = 0.0; yt[i] = 0.0;
+    }
+}
+
+__global__ void k_rc_rows(int m, const Ctrl* __restrict__ c, const int32_t* __restrict__ ptr,
+                          const int32_t* __restrict__ idx, const double* __restrict__ vals,
+                          const double* __restrict__ xbar, const double* __restrict__ ybar,
+                          const double* __restrict__ b, const double* __restrict__ dr, double* axbar, double* bs,
+                          double* ylb_s) {
+    if (c->done || !c->restart) return;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
+        double s = 0.0;
+        for (int k = ptr[i]; k < ptr[i + 1]; ++k) s += vals[k] * xbar[idx[k]];
+        axbar[i] = s;
+        bs[i] = dr[i] * (b[i] - s);
+        ylb_s[i] = -ybar[i] / dr[i];
+    }
+}
+
+__global__ void k_rc_cols(int n, const Ctrl* __restrict__ c, const int32_t* __restrict__ ptr,
+                          const int32_t* __restrict__ idx, const double* __restrict__ vals,
+                          const double* __restrict__ xbar, const double* __restrict__ ybar,
+                          const double* __restrict__ cost, const double* __restrict__ lb, const double* __restrict__ ub,
+                          const double* __restrict__ dc, double* atybar, double* cs, double* ls, double* us) {
+    if (c->done || !c->restart) return;
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+        double s = 0.0;
+        for (int k = ptr[j]; k < ptr[j + 1]; ++k) s += vals[k] * ybar[idx[k]];
+        atybar[j] = s;
+        cs[j] = dc[j] * (cost[j] + s);
+        ls[j] = (lb[j] - xbar[j]) / dc[j];
+        us[j] = (ub[j] - xbar[j]) / dc[j];
+    }
 }
 
 int pick_lanes(double mean_len, int requested) {
@@ -549,9 +637,10 @@ void launch_iter(int mode, int L, int R, unsigned grid, int tb, cudaStream_t s, 
     else launch_iter_LR<VT, GT, 1, M_PLAIN, PRIMAL>(L, grid, tb, s, a, it);
 }
 
-void launch_kkt(int Lr, int Lc, unsigned gr, unsigned gc, cudaStream_t s, const DevLP& lp, HalpernWork* w, Ctrl* ctrl) {
-#define KR(LL) k_kkt_rows<LL><<<gr, TB, 0, s>>>(lp.m, lp.rowptr.p, lp.colidx.p, w->sv64.p, w->xt.p, w->yt.p, lp.b.p, lp.is_eq.p, w->dr.p, ctrl)
-#define KC(LL) k_kkt_cols<LL><<<gc, TB, 0, s>>>(lp.n, lp.t_rowptr.p, lp.t_colidx.p, w->stv64.p, w->yt.p, w->xt.p, lp.c.p, lp.lb.p, lp.ub.p, w->dc.p, ctrl)
+void launch_kkt(int Lr, int Lc, unsigned gr, unsigned gc, cudaStream_t s, const DevLP& lp, HalpernWork* w,
+                const KktMap& map, Ctrl* ctrl) {
+#define KR(LL) k_kkt_rows<LL><<<gr, TB, 0, s>>>(lp.m, lp.rowptr.p, lp.colidx.p, w->sv64.p, w->xt.p, w->yt.p, lp.b.p, lp.is_eq.p, w->dr.p, map, ctrl)
+#define KC(LL) k_kkt_cols<LL><<<gc, TB, 0, s>>>(lp.n, lp.t_rowptr.p, lp.t_colidx.p, w->stv64.p, w->yt.p, w->xt.p, lp.c.p, lp.lb.p, lp.ub.p, w->dc.p, map, ctrl)
     switch (Lr) { case 1: KR(1); break; case 2: KR(2); break; case 4: KR(4); break; case 8: KR(8); break; case 16: KR(16); break; default: KR(32); }
     switch (Lc) { case 1: KC(1); break; case 2: KC(2); break; case 4: KC(4); break; case 8: KC(8); break; case 16: KC(16); break; default: KC(32); }
 #undef KR
@@ -645,6 +734,20 @@ struct Ops<float> {
     static float* xh(HalpernWork* w) { return w->xh32.p; }
 };
 
+// Arguments of the primal kernel (A^T y over the CSR of A^T, updates x) and of the
+// dual kernel (A xh over the CSR of A, updates y; with re-centring its sign bound
+// on <= rows is the shifted ylb_s).
+template <typename MT>
+IterArgs<MT, double> primal_args(const DevLP& L, HalpernWork* w, const b2p_params* p) {
+    return {L.t_rowptr.p, L.t_colidx.p, Ops<MT>::stv(w), w->y.p, w->c64.p, w->l64.p, w->u64.p, nullptr, nullptr,
+            w->x.p, Ops<MT>::xh(w), w->xa.p, w->xt.p, w->ctrl.p, L.n, p->reflection};
+}
+template <typename MT>
+IterArgs<MT, MT> dual_args(const DevLP& L, HalpernWork* w, const b2p_params* p) {
+    return {L.rowptr.p, L.colidx.p, Ops<MT>::sv(w), Ops<MT>::xh(w), w->b64.p, nullptr, nullptr, L.is_eq.p,
+            w->recenter ? w->ylb_s.p : nullptr, w->y.p, nullptr, w->ya.p, w->yt.p, w->ctrl.p, L.m, p->reflection};
+}
+
 // One resident wave: 2048 / tb CTAs per SM, each owning a contiguous row range.
 inline unsigned iter_grid(int64_t rows, int L, int R, int tb, int sm_count) {
     return grid_for((rows * L + R - 1) / R, tb, sm_count, 2048 / tb);
@@ -669,10 +772,8 @@ int autotune_shapes(Ctx* ctx, HalpernWork* w, const b2p_params* p) {
     cudaStream_t s = ctx->stream;
     const int m = L.m, n = L.n;
     Ctrl* ctrl = w->ctrl.p;
-    IterArgs<MT, double> pa{L.t_rowptr.p, L.t_colidx.p, Ops<MT>::stv(w), w->y.p, w->c64.p, w->l64.p, w->u64.p,
-                            nullptr, w->x.p, Ops<MT>::xh(w), w->xa.p, w->xt.p, ctrl, n, p->reflection};
-    IterArgs<MT, MT> da{L.rowptr.p, L.colidx.p, Ops<MT>::sv(w), Ops<MT>::xh(w), w->b64.p, nullptr, nullptr, L.is_eq.p,
-                        w->y.p, nullptr, w->ya.p, w->yt.p, ctrl, m, p->reflection};
+    const IterArgs<MT, double> pa = primal_args<MT>(L, w, p);
+    const IterArgs<MT, MT> da = dual_args<MT>(L, w, p);
     cudaEvent_t e0, e1;
     B2P_CUDA(ctx, cudaEventCreate(&e0));
     B2P_CUDA(ctx, cudaEventCreate(&e1));
@@ -728,10 +829,8 @@ int run_chunks(Ctx* ctx, HalpernWork* w, const b2p_params* p, double time_limit_
     unsigned grR = iter_grid(m, Lr, Rr, Tr, ctx->sm_count), gcR = iter_grid(n, Lc, Rc, Tc, ctx->sm_count);
     unsigned gkr = iter_grid(m, Lr, 1, TB, ctx->sm_count), gkc = iter_grid(n, Lc, 1, TB, ctx->sm_count);
     Ctrl* ctrl = w->ctrl.p;
-    IterArgs<MT, double> pa{L.t_rowptr.p, L.t_colidx.p, Ops<MT>::stv(w), w->y.p, w->c64.p, w->l64.p, w->u64.p,
-                            nullptr, w->x.p, Ops<MT>::xh(w), w->xa.p, w->xt.p, ctrl, n, p->reflection};
-    IterArgs<MT, MT> da{L.rowptr.p, L.colidx.p, Ops<MT>::sv(w), Ops<MT>::xh(w), w->b64.p, nullptr, nullptr, L.is_eq.p,
-                        w->y.p, nullptr, w->ya.p, w->yt.p, ctrl, m, p->reflection};
+    const IterArgs<MT, double> pa = primal_args<MT>(L, w, p);
+    const IterArgs<MT, MT> da = dual_args<MT>(L, w, p);
     auto chunk = [&]() {
         for (int i = 0; i < K; ++i) {
             int mode = (i == 0) ? M_FIRST : (i == K - 1 ? M_CHECK : M_PLAIN);
@@ -743,10 +842,24 @@ int run_chunks(Ctx* ctx, HalpernWork* w, const b2p_params* p, double time_limit_
                 launch_iter<MT, MT, false>(mode, Lr, 1, gr, Tr, s, da, i);
             }
         }
-        launch_kkt(Lr, Lc, gkr, gkc, s, L, w, ctrl);
+        const KktMap map = w->recenter ? KktMap{w->xbar.p, w->ybar.p, w->axbar.p, w->atybar.p}
+                                       : KktMap{nullptr, nullptr, nullptr, nullptr};
+        launch_kkt(Lr, Lc, gkr, gkc, s, L, w, map, ctrl);
         k_control<<<1, 1, 0, s>>>(ctrl);
-        k_restart<<<grid_for(std::max(m, n), TB, ctx->sm_count, 8), TB, 0, s>>>(m, n, ctrl, w->x.p, w->xa.p, w->xt.p,
-                                                                               w->y.p, w->ya.p, w->yt.p, nullptr);
+        const unsigned gv = grid_for(std::max(m, n), TB, ctx->sm_count, 8);
+        if (w->recenter) {
+            k_rc_update<<<gv, TB, 0, s>>>(m, n, ctrl, w->dr.p, w->dc.p, w->xbar.p, w->ybar.p, w->x.p, w->xa.p, w->xt.p,
+                                          w->y.p, w->ya.p, w->yt.p);
+            k_rc_rows<<<grid_for(m, TB, ctx->sm_count, 8), TB, 0, s>>>(m, ctrl, L.rowptr.p, L.colidx.p, L.vals.p,
+                                                                      w->xbar.p, w->ybar.p, L.b.p, w->dr.p,
+                                                                      w->axbar.p, w->b64.p, w->ylb_s.p);
+            k_rc_cols<<<grid_for(n, TB, ctx->sm_count, 8), TB, 0, s>>>(n, ctrl, L.t_rowptr.p, L.t_colidx.p, L.t_vals.p,
+                                                                      w->xbar.p, w->ybar.p, L.c.p, L.lb.p, L.ub.p,
+                                                                      w->dc.p, w->atybar.p, w->c64.p, w->l64.p,
+                                                                      w->u64.p);
+        } else {
+            k_restart<<<gv, TB, 0, s>>>(m, n, ctrl, w->x.p, w->xa.p, w->xt.p, w->y.p, w->ya.p, w->yt.p, nullptr);
+        }
     };
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
@@ -815,6 +928,19 @@ int solve_T(Ctx* ctx, HalpernWork* w, const b2p_params* p, const double* x0, con
     } else {
         B2P_CUDA(ctx, w->xh64.reserve(n));
     }
+    // re-centring (FP64 iterative refinement at every restart): on by default for the
+    // mixed engine, off for FP64; refinement_rounds > 0 forces it on, 0 off
+    w->recenter = p->refinement_rounds > 0 || (p->refinement_rounds < 0 && mixed);
+    if (w->recenter) {
+        for (auto* b : {&w->xbar, &w->atybar}) {
+            B2P_CUDA(ctx, b->reserve(n));
+            B2P_CUDA(ctx, cudaMemsetAsync(b->p, 0, sizeof(double) * n, s));
+        }
+        for (auto* b : {&w->ybar, &w->axbar, &w->ylb_s}) {
+            B2P_CUDA(ctx, b->reserve(m));
+            B2P_CUDA(ctx, cudaMemsetAsync(b->p, 0, sizeof(double) * m, s));
+        }
+    }
     int st = prepare_scaling(ctx, w, p->ruiz_iterations, mixed);
     if (st) return st;
     double sig2 = 0.0;
@@ -847,7 +973,7 @@ int solve_T(Ctx* ctx, HalpernWork* w, const b2p_params* p, const double* x0, con
         y0d = w->tmp_m.p;
     }
     k_init_iterates<<<grid_for(std::max(m, n), TB, ctx->sm_count), TB, 0, s>>>(
-        m, n, w->l64.p, w->u64.p, x0d, y0d, w->dr.p, w->dc.p, L.is_eq.p, w->x.p, w->xa.p, w->xt.p, w->y.p, w->ya.p,
+        m, n, w->l64.p, w->u64.p, x0d, y0d, w->dr.p, w->dc.p, L.is_eq.p, nullptr, w->x.p, w->xa.p, w->xt.p, w->y.p, w->ya.p,
         w->yt.p, nullptr);
     B2P_LAUNCH(ctx);
     ctx->launches += 1;
@@ -867,6 +993,10 @@ int solve_T(Ctx* ctx, HalpernWork* w, const b2p_params* p, const double* x0, con
     hc.K = p->check_every;
     hc.first_after_restart = 1;
     hc.status = B2P_STATUS_MAX_ITERATIONS;
+    hc.pscale = 1.0;
+    hc.dscale = 1.0;
+    hc.inner_tol = 0.0;
+    hc.r_first = 0.0;
     B2P_CUDA(ctx, cudaMemcpyAsync(w->ctrl.p, &hc, sizeof(Ctrl), cudaMemcpyHostToDevice, s));
     {
         const long long before = w->tuned_key;
@@ -874,7 +1004,7 @@ int solve_T(Ctx* ctx, HalpernWork* w, const b2p_params* p, const double* x0, con
         if (st) return st;
         if (before != w->tuned_key && w->tuned_key >= 0) {  // the trial iterations moved the iterates: reset
             k_init_iterates<<<grid_for(std::max(m, n), TB, ctx->sm_count), TB, 0, s>>>(
-                m, n, w->l64.p, w->u64.p, x0d, y0d, w->dr.p, w->dc.p, L.is_eq.p, w->x.p, w->xa.p, w->xt.p, w->y.p,
+                m, n, w->l64.p, w->u64.p, x0d, y0d, w->dr.p, w->dc.p, L.is_eq.p, nullptr, w->x.p, w->xa.p, w->xt.p, w->y.p,
                 w->ya.p, w->yt.p, nullptr);
             B2P_LAUNCH(ctx);
             ctx->launches += 1;
@@ -902,10 +1032,12 @@ int solve_T(Ctx* ctx, HalpernWork* w, const b2p_params* p, const double* x0, con
     r->rel_kkt = std::max(fin.rel_p, std::max(fin.rel_d, fin.rel_g));
     r->primal_weight = fin.omega;
     r->step_size = eta;
+    r->refinement_rounds_done = w->recenter ? (int)fin.restarts : 0;
     if (x_out || y_out) {
         double t0 = now_ms();
-        k_unscale<<<grid_for(std::max(m, n), TB, ctx->sm_count), TB, 0, s>>>(m, n, w->xt.p, w->yt.p, w->dr.p, w->dc.p,
-                                                                           w->tmp_n.p, w->tmp_m.p);
+        k_unscale<<<grid_for(std::max(m, n), TB, ctx->sm_count), TB, 0, s>>>(
+            m, n, w->xt.p, w->yt.p, w->dr.p, w->dc.p, w->recenter ? w->xbar.p : nullptr,
+            w->recenter ? w->ybar.p : nullptr, w->tmp_n.p, w->tmp_m.p);
         B2P_LAUNCH(ctx);
         ctx->launches += 1;
         if (x_out) B2P_CUDA(ctx, cudaMemcpyAsync(x_out, w->tmp_n.p, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
@@ -932,10 +1064,8 @@ int kernel_timing_T(Ctx* ctx, HalpernWork* w, const b2p_params* p, int reps, dou
     Ctrl open = saved;
     open.done = 0;
     B2P_CUDA(ctx, cudaMemcpyAsync(ctrl, &open, sizeof(Ctrl), cudaMemcpyHostToDevice, s));
-    IterArgs<MT, double> pa{L.t_rowptr.p, L.t_colidx.p, Ops<MT>::stv(w), w->y.p, w->c64.p, w->l64.p, w->u64.p,
-                            nullptr, w->x.p, Ops<MT>::xh(w), w->xa.p, w->xt.p, ctrl, n, p->reflection};
-    IterArgs<MT, MT> da{L.rowptr.p, L.colidx.p, Ops<MT>::sv(w), Ops<MT>::xh(w), w->b64.p, nullptr, nullptr, L.is_eq.p,
-                        w->y.p, nullptr, w->ya.p, w->yt.p, ctrl, m, p->reflection};
+    const IterArgs<MT, double> pa = primal_args<MT>(L, w, p);
+    const IterArgs<MT, MT> da = dual_args<MT>(L, w, p);
     cudaEvent_t e[3];
     for (auto& x : e) B2P_CUDA(ctx, cudaEventCreate(&x));
     double tp = 0, td = 0;

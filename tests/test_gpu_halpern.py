@@ -101,3 +101,44 @@ def test_halpern_time_limit(ctx, lps):
     ctx.upload(std)
     res, _, _ = ctx.solve(engine="halpern", precision="fp64", eps=0.0, max_iterations=10**8, time_limit_s=0.2)
     assert res["status"] == "INTERRUPTED"
+
+
+def test_mixed_refinement_ill_conditioned(ctx, golden, lps):
+    """FP32 matrix values with FP64 re-centring at restarts reach 1e-8 on the badly scaled LP
+    (FP32 without it stalls near 1e-5).  Here ||b|| ~ 1e9, so a 1e-8 relative primal residual
+    still allows absolute row violations of order 10 and the objective is pinned only to ~1e-5;
+    at 1e-10 it is pinned to 1e-6."""
+    std = lps["ill_small"].standard()
+    ctx.upload(std)
+    z = golden["highs"]["ill_small"]
+    res, x, y = ctx.solve(engine="halpern", precision="fp32", eps=1e-8, max_iterations=400000)
+    assert res["status"] == "OPTIMAL", res
+    assert res["refinement_rounds_done"] > 0
+    k = pdlp_oracle.kkt(std, x, y)
+    assert k["rel_kkt"] <= 1.05e-8, k
+    assert abs(k["pobj"] - z) <= 1e-5 * abs(z), (k["pobj"], z)
+    res, x, y = ctx.solve(engine="halpern", precision="fp32", eps=1e-10, max_iterations=1000000)
+    assert res["status"] == "OPTIMAL", res
+    k = pdlp_oracle.kkt(std, x, y)
+    assert k["rel_kkt"] <= 1.05e-10, k
+    assert abs(k["pobj"] - z) <= 1e-6 * abs(z), (k["pobj"], z)
+
+
+def test_mixed_refinement_tight_tolerance(ctx, golden, lps):
+    std = lps["rs_c0"].standard()
+    ctx.upload(std)
+    res, x, y = ctx.solve(engine="halpern", precision="fp32", eps=1e-9, max_iterations=200000)
+    assert res["status"] == "OPTIMAL", res
+    k = pdlp_oracle.kkt(std, x, y)
+    assert k["rel_kkt"] <= 1.05e-9
+    assert abs(k["pobj"] - golden["highs"]["rs_c0"]) <= 1e-8 * abs(golden["highs"]["rs_c0"])
+
+
+def test_mixed_without_refinement_matches_fp64_iterations_at_1e6(ctx, lps):
+    """At 1e-6 the FP32 values cost no iterations: same count as FP64 within one chunk."""
+    std = lps["rs_c0"].standard()
+    ctx.upload(std)
+    r64, _, _ = ctx.solve(engine="halpern", precision="fp64", eps=1e-6)
+    r32, _, _ = ctx.solve(engine="halpern", precision="fp32", eps=1e-6)
+    assert r64["status"] == r32["status"] == "OPTIMAL"
+    assert abs(r64["iterations"] - r32["iterations"]) <= 2 * 64
