@@ -234,6 +234,13 @@ int b2p_mlp_create(void* ctx, int in_dim, int hidden, int out_dim, uint64_t seed
  * host).  loss_out (optional) receives the mean squared error of the epoch. */
 int b2p_mlp_train_epoch(void* ctx, const float* X, const float* Y, int N, int batch, float lr, float* loss_out);
 int b2p_mlp_infer(void* ctx, const float* X, int N, float* Y_out);
+/* All parameters as one FP32 vector: W1 [hidden x in], b1 [hidden], W2 [hidden x
+ * hidden], b2 [hidden], W3 [out x hidden], b3 [out] (row-major). */
+int b2p_mlp_get_params(void* ctx, float* flat);
+int b2p_mlp_set_params(void* ctx, const float* flat);
+/* Mean-squared-error loss of one batch and its gradient (flat layout as above),
+ * computed by the same tensor-core forward / backward the training step uses. */
+int b2p_mlp_gradient(void* ctx, const float* X, const float* Y, int N, float* loss_out, float* grad_flat);
 /* Raw BF16 GEMM on the tensor cores, for tests: C(MxN, fp32) = op(A) op(B),
  * A is M x K (trans_a = 0) or K x M (trans_a = 1) bf16 row-major, B is K x N
  * (trans_b = 0) or N x K (trans_b = 1).  Host buffers (bf16 as uint16). */

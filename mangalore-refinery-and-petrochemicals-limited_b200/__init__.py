@@ -95,6 +95,9 @@ SIGNATURES = {
     "b2p_mlp_create": (C.c_int, [_P, C.c_int, C.c_int, C.c_int, C.c_uint64]),
     "b2p_mlp_train_epoch": (C.c_int, [_P, _F32P, _F32P, C.c_int, C.c_int, C.c_float, C.POINTER(C.c_float)]),
     "b2p_mlp_infer": (C.c_int, [_P, _F32P, C.c_int, _F32P]),
+    "b2p_mlp_get_params": (C.c_int, [_P, _F32P]),
+    "b2p_mlp_set_params": (C.c_int, [_P, _F32P]),
+    "b2p_mlp_gradient": (C.c_int, [_P, _F32P, _F32P, C.c_int, C.POINTER(C.c_float), _F32P]),
     "b2p_gemm_bf16": (C.c_int, [_P, C.c_int, C.c_int, C.c_int, _U16P, C.c_int, _U16P, C.c_int, _F32P]),
 }
 
@@ -292,6 +295,7 @@ class Context:
     def mlp_create(self, in_dim, hidden, out_dim, seed=0):
         self._check(lib().b2p_mlp_create(self._h, in_dim, hidden, out_dim, seed))
         self.mlp_out = out_dim
+        self.mlp_dims = (in_dim, hidden, out_dim)
 
     def mlp_train_epoch(self, X, Y, batch=256, lr=1e-3):
         loss = C.c_float()
@@ -305,6 +309,28 @@ class Context:
         out = np.zeros((X.shape[0], self.mlp_out), np.float32)
         self._check(lib().b2p_mlp_infer(self._h, X, X.shape[0], out))
         return out
+
+    def mlp_param_count(self):
+        i, h, o = self.mlp_dims
+        return h * i + h + h * h + h + o * h + o
+
+    def mlp_get_params(self):
+        out = np.zeros(self.mlp_param_count(), np.float32)
+        self._check(lib().b2p_mlp_get_params(self._h, out))
+        return out
+
+    def mlp_set_params(self, flat):
+        flat = np.ascontiguousarray(flat, np.float32)
+        assert flat.size == self.mlp_param_count()
+        self._check(lib().b2p_mlp_set_params(self._h, flat))
+
+    def mlp_gradient(self, X, Y):
+        X = np.ascontiguousarray(X, np.float32)
+        Y = np.ascontiguousarray(Y, np.float32)
+        g = np.zeros(self.mlp_param_count(), np.float32)
+        loss = C.c_float()
+        self._check(lib().b2p_mlp_gradient(self._h, X, Y, X.shape[0], C.byref(loss), g))
+        return loss.value, g
 
     def gemm_bf16(self, A, B, trans_a=False, trans_b=False):
         """A, B given as uint16 bf16 bit patterns (row-major)."""
