@@ -222,10 +222,11 @@ int b2p_batch_upload(void* ctx, int nmat, const int32_t* mat_m, const int32_t* m
                      const double* ub, const uint8_t* is_eq);
 /* Solve all instances with the Halpern engine.  x0/y0 optional warm starts
  * (concatenated like c / b), omega0 optional per-instance primal weights.
- * Outputs (optional): per-instance status, iterations, rel KKT; concatenated x, y. */
+ * Outputs (optional): per-instance status, iterations, rel KKT and final primal
+ * weight; concatenated x, y. */
 int b2p_batch_solve(void* ctx, const b2p_params* params, const double* x0, const double* y0, const double* omega0,
-                    int32_t* status_out, int64_t* iters_out, double* kkt_out, double* x_out, double* y_out,
-                    b2p_result* summary);
+                    int32_t* status_out, int64_t* iters_out, double* kkt_out, double* omega_out, double* x_out,
+                    double* y_out, b2p_result* summary);
 
 /* ---- learned warm start: MLP in -> h -> h -> out, GELU, BF16 weights and
  *      activations, FP32 accumulation on the tcgen05 tensor cores ---- */

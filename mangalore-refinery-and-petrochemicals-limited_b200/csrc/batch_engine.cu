@@ -68,6 +68,8 @@ struct BatchWork {
     DBuf<double> b, c, lb, ub, bnorm, cnorm;
     DBuf<uint8_t> is_eq;
     DBuf<double> bs, cs, ls, us, x, xa, xt, y, ya, yt;  // scaled vectors and FP64 iterates
+    bool recenter = false;
+    DBuf<double> xbar, atybar, ybar, axbar, ylb_s;      // re-centring state (per instance)
     DBuf<InstCtrl> ictrl;
     DBuf<int32_t> active, active2, counters;  // counters[0]=head, [1]=active count
     std::vector<int32_t> h_inst_mat, order;
@@ -93,13 +95,18 @@ struct BArgs {
     const int64_t *x_off, *y_off;
     const double *b, *c, *lb, *ub, *bnorm, *cnorm;
     const uint8_t* is_eq;
-    const double *bs, *cs, *ls, *us;
+    double *bs, *cs, *ls, *us;  // scaled problem vectors (rewritten by re-centring)
     double *x, *xa, *xt, *y, *ya, *yt;
     InstCtrl* ictrl;
     const int32_t* active;
     int32_t* counters;
     // parameters
     double eps, beta_s, beta_n, beta_a, rho;
+    // FP64 re-centring at restarts (as in the single-LP engine): per-instance centre in
+    // the original space, A xbar, A^T ybar, shifted dual bound; original FP64 values
+    int recenter;
+    const double *vals, *t_vals;
+    double *xbar, *ybar, *axbar, *atybar, *ylb_s;
     long long max_iter;
     int K;
 };
@@ -139,7 +146,7 @@ __global__ void __launch_bounds__(512) k_batch_chunk(BArgs a, int chunk) {
     const int lane = tid & 31, warp = tid >> 5, nwarps = nt >> 5;
     const MT* sv = (const MT*)a.sv;
     const MT* stv = (const MT*)a.stv;
-    const double *bs = a.bs, *cs = a.cs, *ls = a.ls, *us = a.us;
+    double *bs = a.bs, *cs = a.cs, *ls = a.ls, *us = a.us;
     double *xg = a.x, *xag = a.xa, *xtg = a.xt, *yg = a.y, *yag = a.ya, *ytg = a.yt;
     const int active_count = a.counters[1];
     while (true) {
@@ -217,7 +224,10 @@ __global__ void __launch_bounds__(512) k_batch_chunk(BArgs a, int chunk) {
                     if (valid && sub == 0) {
                         const double yi = ys[i];
                         double yt = yi + sigma * (s - bs[yo + i]);
-                        if (!a.is_eq[yo + i] && yt < 0.0) yt = 0.0;
+                        if (!a.is_eq[yo + i]) {
+                            const double lbv = a.recenter ? a.ylb_s[yo + i] : 0.0;
+                            if (yt < lbv) yt = lbv;
+                        }
                         const double ya = yag[yo + i];
                         ys[i] = wk * ((1.0 + rho) * yt - rho * yi) + wa * ya;
                         if (first || check) {
@@ -274,10 +284,11 @@ __global__ void __launch_bounds__(512) k_batch_chunk(BArgs a, int chunk) {
                     for (int o = LR / 2; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
                     if (valid && sub == 0) {
                         const double dri = a.dr[ro + i];
-                        double rp = s / dri - a.b[yo + i];
+                        const double ax = (a.recenter ? a.axbar[yo + i] : 0.0) + s / dri;
+                        double rp = ax - a.b[yo + i];
                         if (!a.is_eq[yo + i]) rp = fmax(rp, 0.0);
                         kk2[0] += rp * rp;
-                        kk2[1] += a.b[yo + i] * (dri * ytg[yo + i]);
+                        kk2[1] += a.b[yo + i] * ((a.recenter ? a.ybar[yo + i] : 0.0) + dri * ytg[yo + i]);
                     }
                 }
             }
@@ -297,12 +308,12 @@ __global__ void __launch_bounds__(512) k_batch_chunk(BArgs a, int chunk) {
                     if (valid && sub == 0) {
                         const double dcj = a.dc[co + j];
                         const double cj = a.c[xo + j], lj = a.lb[xo + j], uj = a.ub[xo + j];
-                        const double g = cj + s / dcj;
+                        const double g = cj + (a.recenter ? a.atybar[xo + j] : 0.0) + s / dcj;
                         const bool fl = isfinite(lj), fu = isfinite(uj);
                         const double lam = (fl && fu) ? g : (fl ? fmax(g, 0.0) : (fu ? fmin(g, 0.0) : 0.0));
                         const double rd = g - lam;
                         kk2[2] += rd * rd;
-                        kk2[3] += cj * (dcj * xtg[xo + j]);
+                        kk2[3] += cj * ((a.recenter ? a.xbar[xo + j] : 0.0) + dcj * xtg[xo + j]);
                         if (lam > 0.0) kk2[4] += lam * lj;
                         else if (lam < 0.0) kk2[4] += lam * uj;
                     }
@@ -346,7 +357,7 @@ __global__ void __launch_bounds__(512) k_batch_chunk(BArgs a, int chunk) {
                 s_flags[0] = sc.done;
             }
             __syncthreads();
-            if (s_flags[1]) {  // restart: z <- anchor <- T(z)
+            if (s_flags[1] && !a.recenter) {  // restart: z <- anchor <- T(z)
                 for (int j = tid; j < n; j += nt) {
                     const double v = xtg[xo + j];
                     xg[xo + j] = v;
@@ -356,6 +367,42 @@ __global__ void __launch_bounds__(512) k_batch_chunk(BArgs a, int chunk) {
                     const double v = ytg[yo + i];
                     ys[i] = v;
                     yag[yo + i] = v;
+                }
+            } else if (s_flags[1]) {
+                // restart with re-centring: the LP is rewritten around T(z) (an exact change of
+                // variables) with b - A xbar and c + A^T ybar from the FP64 original matrix
+                for (int j = tid; j < n; j += nt) {
+                    a.xbar[xo + j] += a.dc[co + j] * xtg[xo + j];
+                    xg[xo + j] = 0.0;
+                    xag[xo + j] = 0.0;
+                    xtg[xo + j] = 0.0;
+                }
+                for (int i = tid; i < m; i += nt) {
+                    a.ybar[yo + i] += a.dr[ro + i] * ytg[yo + i];
+                    ys[i] = 0.0;
+                    yag[yo + i] = 0.0;
+                    ytg[yo + i] = 0.0;
+                }
+                __syncthreads();
+                for (int i = tid; i < m; i += nt) {
+                    const int64_t gi = ro + i;
+                    double s = 0.0;
+                    for (int e = a.rowptr[gi]; e < a.rowptr[gi + 1]; ++e) s += a.vals[e] * a.xbar[xo + a.colidx[e] - co];
+                    const double dri = a.dr[gi];
+                    a.axbar[yo + i] = s;
+                    bs[yo + i] = dri * (a.b[yo + i] - s);
+                    a.ylb_s[yo + i] = -a.ybar[yo + i] / dri;
+                }
+                for (int j = tid; j < n; j += nt) {
+                    const int64_t gj = co + j;
+                    double s = 0.0;
+                    for (int e = a.t_rowptr[gj]; e < a.t_rowptr[gj + 1]; ++e)
+                        s += a.t_vals[e] * a.ybar[yo + a.t_colidx[e] - ro];
+                    const double dcj = a.dc[gj];
+                    a.atybar[xo + j] = s;
+                    cs[xo + j] = dcj * (a.c[xo + j] + s);
+                    ls[xo + j] = (a.lb[xo + j] - a.xbar[xo + j]) / dcj;
+                    us[xo + j] = (a.ub[xo + j] - a.xbar[xo + j]) / dcj;
                 }
             }
             __syncthreads();
@@ -597,13 +644,16 @@ __global__ void k_batch_unscale(int count, const int32_t* __restrict__ inst_mat,
                                 const int64_t* __restrict__ col_off, const int64_t* __restrict__ x_off,
                                 const int64_t* __restrict__ y_off, const double* __restrict__ dr,
                                 const double* __restrict__ dc, const T* __restrict__ xt, const T* __restrict__ yt,
+                                const double* __restrict__ xbar, const double* __restrict__ ybar,
                                 double* __restrict__ xo_, double* __restrict__ yo_) {
     for (int inst = blockIdx.x; inst < count; inst += gridDim.x) {
         const int k = inst_mat[inst];
         const int m = mat_m[k], n = mat_n[k];
         const int64_t ro = row_off[k], co = col_off[k], xo = x_off[inst], yo = y_off[inst];
-        for (int j = threadIdx.x; j < n; j += blockDim.x) xo_[xo + j] = dc[co + j] * (double)xt[xo + j];
-        for (int i = threadIdx.x; i < m; i += blockDim.x) yo_[yo + i] = dr[ro + i] * (double)yt[yo + i];
+        for (int j = threadIdx.x; j < n; j += blockDim.x)
+            xo_[xo + j] = (xbar ? xbar[xo + j] : 0.0) + dc[co + j] * (double)xt[xo + j];
+        for (int i = threadIdx.x; i < m; i += blockDim.x)
+            yo_[yo + i] = (ybar ? ybar[yo + i] : 0.0) + dr[ro + i] * (double)yt[yo + i];
     }
 }
 
@@ -711,6 +761,14 @@ BArgs make_args(BatchWork* w, const b2p_params* p, const void* sv, const void* s
     a.rho = p->reflection;
     a.max_iter = p->max_iterations;
     a.K = p->check_every;
+    a.recenter = w->recenter ? 1 : 0;
+    a.vals = w->vals.p;
+    a.t_vals = w->t_vals.p;
+    a.xbar = w->xbar.p;
+    a.ybar = w->ybar.p;
+    a.axbar = w->axbar.p;
+    a.atybar = w->atybar.p;
+    a.ylb_s = w->ylb_s.p;
     return a;
 }
 
@@ -791,10 +849,12 @@ int autotune(Ctx* ctx, BatchWork* w, const b2p_params* p, TuneCfg* best) {
 
 template <typename MT>
 int batch_run(Ctx* ctx, BatchWork* w, const b2p_params* p, const double* x0, const double* y0, const double* omega0,
-              int32_t* status_out, int64_t* iters_out, double* kkt_out, double* x_out, double* y_out, b2p_result* sum) {
+              int32_t* status_out, int64_t* iters_out, double* kkt_out, double* omega_out, double* x_out, double* y_out,
+              b2p_result* sum) {
     cudaStream_t s = ctx->stream;
     double t_start = now_ms();
     const int64_t IN = w->inst_n, IM = w->inst_m;
+    w->recenter = false;  // autotune trials run without re-centring (its buffers are set up below)
     // lanes per column / row, threads per CTA, chunk length: explicit, cached or tuned now
     TuneCfg cfg = {4, 16, 256, 2048};
     if (p->lanes_per_row > 0) {
@@ -820,6 +880,18 @@ int batch_run(Ctx* ctx, BatchWork* w, const b2p_params* p, const double* x0, con
     }
     int st = init_instances(ctx, w, x0 ? dx0.p : nullptr, y0 ? dy0.p : nullptr, omega0 ? dom.p : nullptr);
     if (st) return st;
+    // re-centring: on by default for the mixed engine (refinement_rounds < 0), forced by > 0
+    w->recenter = p->refinement_rounds > 0 || (p->refinement_rounds < 0 && sizeof(MT) == 4);
+    if (w->recenter) {
+        for (auto* b : {&w->xbar, &w->atybar}) {
+            B2P_CUDA(ctx, b->reserve(IN));
+            B2P_CUDA(ctx, cudaMemsetAsync(b->p, 0, sizeof(double) * IN, s));
+        }
+        for (auto* b : {&w->ybar, &w->axbar, &w->ylb_s}) {
+            B2P_CUDA(ctx, b->reserve(IM));
+            B2P_CUDA(ctx, cudaMemsetAsync(b->p, 0, sizeof(double) * IM, s));
+        }
+    }
     // active list = all instances, longest first
     B2P_CUDA(ctx, cudaMemcpyAsync(w->active.p, w->order.data(), sizeof(int32_t) * w->count, cudaMemcpyHostToDevice, s));
     int32_t cnt[2] = {0, w->count};
@@ -890,7 +962,8 @@ int batch_run(Ctx* ctx, BatchWork* w, const b2p_params* p, const double* x0, con
         B2P_CUDA(ctx, oy.reserve(IM));
         k_batch_unscale<double><<<std::min(w->count, ctx->sm_count * 8), 256, 0, s>>>(
             w->count, w->inst_mat.p, w->mat_m.p, w->mat_n.p, w->mat_row_off.p, w->mat_col_off.p, w->x_off.p, w->y_off.p,
-            w->dr.p, w->dc.p, w->xt.p, w->yt.p, ox.p, oy.p);
+            w->dr.p, w->dc.p, w->xt.p, w->yt.p, w->recenter ? w->xbar.p : nullptr, w->recenter ? w->ybar.p : nullptr,
+            ox.p, oy.p);
         B2P_LAUNCH(ctx);
         ctx->launches += 1;
         if (x_out) B2P_CUDA(ctx, cudaMemcpyAsync(x_out, ox.p, sizeof(double) * IN, cudaMemcpyDeviceToHost, s));
@@ -906,6 +979,7 @@ int batch_run(Ctx* ctx, BatchWork* w, const b2p_params* p, const double* x0, con
         if (status_out) status_out[i] = stt;
         if (iters_out) iters_out[i] = c.total;
         if (kkt_out) kkt_out[i] = kk;
+        if (omega_out) omega_out[i] = c.omega;
         tot_it += c.total;
         maxit = std::max<int64_t>(maxit, c.total);
         opt += (stt == B2P_STATUS_OPTIMAL);
@@ -1091,8 +1165,8 @@ int b2p_batch_upload(void* p, int nmat, const int32_t* mat_m, const int32_t* mat
 }
 
 int b2p_batch_solve(void* p, const b2p_params* params, const double* x0, const double* y0, const double* omega0,
-                    int32_t* status_out, int64_t* iters_out, double* kkt_out, double* x_out, double* y_out,
-                    b2p_result* summary) {
+                    int32_t* status_out, int64_t* iters_out, double* kkt_out, double* omega_out, double* x_out,
+                    double* y_out, b2p_result* summary) {
     Ctx* ctx = static_cast<Ctx*>(p);
     if (!ctx) return B2P_GPU_UNINITIALIZED;
     if (!ctx->bw) {
@@ -1112,8 +1186,10 @@ int b2p_batch_solve(void* p, const b2p_params* params, const double* x0, const d
     int64_t l0 = ctx->launches;
     double t0 = now_ms();
     int st = pp->precision == B2P_FP64
-                 ? batch_run<double>(ctx, ctx->bw, pp, x0, y0, omega0, status_out, iters_out, kkt_out, x_out, y_out, summary)
-                 : batch_run<float>(ctx, ctx->bw, pp, x0, y0, omega0, status_out, iters_out, kkt_out, x_out, y_out, summary);
+                 ? batch_run<double>(ctx, ctx->bw, pp, x0, y0, omega0, status_out, iters_out, kkt_out, omega_out, x_out,
+                                     y_out, summary)
+                 : batch_run<float>(ctx, ctx->bw, pp, x0, y0, omega0, status_out, iters_out, kkt_out, omega_out, x_out,
+                                    y_out, summary);
     if (summary) {
         summary->solve_time_ms = now_ms() - t0;
         summary->kernel_launches = ctx->launches - l0;

@@ -42,6 +42,21 @@ def test_batch_uneven_all_optimal(ctx, golden, lpgen, precision):
             assert abs(k["pobj"] - z) <= 1e-6 * max(1.0, abs(z)), (i, k["pobj"], z)
 
 
+def test_batch_mixed_refinement_tight(ctx, golden, lpgen):
+    """FP32 matrix values with FP64 re-centring at every restart reach 1e-9 rel KKT."""
+    lps = lpgen.uneven_batch(6, seed=12) + lpgen.uneven_batch(10, m_hi=500, seed=14)
+    stds = upload_lps(ctx, lps)
+    summ, per, x, y = ctx.batch_solve(precision="fp32", eps=1e-9, max_iterations=200000)
+    assert np.all(per["status"] == 0), (per["status"], per["iterations"])
+    assert np.all(np.isfinite(per["omega"])) and np.all(per["omega"] > 0)
+    for i, (s, (xi, yi)) in enumerate(zip(stds, split(stds, x, y))):
+        k = pdlp_oracle.kkt(s, xi, yi)
+        assert k["rel_kkt"] <= 1.05e-9, (i, k)
+        if i < 6:
+            z = golden["highs"][f"batch12_{i}"]
+            assert abs(k["pobj"] - z) <= 1e-8 * max(1.0, abs(z)), (i, k["pobj"], z)
+
+
 def test_batch_matches_single_engine(ctx, lpgen):
     lps = lpgen.uneven_batch(4, seed=31)
     stds = upload_lps(ctx, lps)
