@@ -3,29 +3,51 @@
 // Layout in HBM
 //   * `nmat` constraint matrices concatenated into one block-diagonal CSR with
 //     GLOBAL row/column indices (row_off[k], col_off[k] per matrix) plus its
-//     stable transpose; FP64 originals, FP64 and FP32 scaled copies.
-//   * `count` instances, each naming a matrix; per-instance vectors (b, c, l, u
-//     in FP64 for the KKT; scaled FP32/FP64 copies; iterates x, xa, xt, y, ya,
-//     yt) concatenated at x_off[i] / y_off[i].
+//     stable transpose (FP64 originals and scaled copies: the restart-check KKT
+//     and the re-centring read these).  Rows and columns of every matrix are
+//     renumbered at upload by decreasing length (stable), so that consecutive
+//     32-row / 32-column slices hold rows of nearly equal length.
+//   * the iteration SpMVs read SELL-32 copies of the scaled matrix, one per
+//     orientation: per slice of 32 rows (columns), `len` = the longest row of the
+//     slice, entries stored column-major inside the slice (entry q of lane l at
+//     slice_ptr + 32 q + l, zero-padded), values in the solve's precision and
+//     16-bit LOCAL indices (an instance whose iterates fit in shared memory has
+//     m, n < 65536).  A warp reads 32 consecutive values and 32 consecutive
+//     indices per step: coalesced, no per-row pointers, no divergence.
+//   * `count` instances, each naming a matrix; b, c, l, u in FP64 (internal
+//     order; KKT and re-centring); per column one packed record {scaled cost,
+//     lower, upper, Halpern anchor} and per row one {scaled rhs, dual lower
+//     bound, anchor} in the solve's precision (16 bytes each in FP32: one
+//     vector load); iterates x, y and the check-point copies xt, yt.  All
+//     concatenated at x_off[i] / y_off[i]; warm starts and answers are mapped
+//     between external and internal order on the device.
 // Execution
 //   * one CTA owns one instance at a time (persistent grid, work queue sorted by
 //     nnz descending = longest-first).  The gathered operands of both SpMVs --
-//     y (FP64, also the dual iterate) for A^T y and xh for A xh -- live in shared
-//     memory; x and the anchors stay in global memory, touched only by their
-//     owning lane.  A PDHG iteration is: primal phase (columns, LC lanes each) |
-//     barrier | dual phase (rows, LR lanes each) | barrier, with matrix entries
-//     streamed from L2/HBM and every gather served from shared memory.
-//   * precision as in the single-LP engine: MT (float = mixed, double = FP64) is
-//     the storage type of the scaled matrix values and of xh; iterates, sums,
-//     scaling and the KKT are FP64.
+//     y (also the dual iterate) for A^T y and xh for A xh -- live in shared
+//     memory; x and the packed records stay in global memory, touched only by
+//     their owning thread.  A PDHG iteration is: primal phase (one thread per
+//     column, one warp per column slice) | barrier | dual phase (one thread per
+//     row) | barrier.  A slice longer than kLongSlice entries per lane is summed
+//     by the whole warp over the CSR copy instead (one dense row cannot stall
+//     its slice).  Control scalars are private copies in every thread; the CTA
+//     only meets in shared memory at restart-check iterations.
+//   * precision MT (float = mixed, double = FP64) is the type of the scaled
+//     matrix values, the packed records, the iterates and the SpMV sums.  FP64 is
+//     kept for the scaling factors, the squared-residual sums, the KKT of the
+//     original instance every K iterations, and the re-centring: the mixed
+//     engine starts every restart epoch at an FP64 centre (xbar, ybar) and
+//     solves the shifted problem rhs b - A xbar, cost c + A^T ybar, bounds
+//     l - xbar, u - xbar, dual bound -ybar, rebuilt from the FP64 matrix, so
+//     the FP32 iterates only carry the correction (iterative refinement).
 //   * per instance: own step size (from its matrix), primal weight, Halpern
 //     counter, restart state, FP64 KKT every K iterations (block reductions in a
 //     fixed order: deterministic), own termination.
 //   * a launch runs every active instance for up to `chunk` iterations; a
-//     compaction kernel drops finished instances; [reset, chunk, compact] is
+//     compaction kernel drops finished instances; [chunk, compact] x 2 is
 //     captured as a CUDA graph and replayed until no instance is active.
-//   * lanes per column / row, block size and chunk length come from an
-//     autotuner that times candidates on a sample of the batch (cached on disk).
+//   * block size comes from an autotuner that times the candidates on a sample
+//     of the batch (cached on disk).
 #include <cub/cub.cuh>
 
 #include <algorithm>
@@ -53,23 +75,30 @@ struct InstCtrl {
 struct BatchWork {
     int nmat = 0, count = 0;
     int64_t tot_m = 0, tot_n = 0, nnz = 0, inst_m = 0, inst_n = 0;
-    // matrices
+    // matrices (internal numbering)
     DBuf<int32_t> rowptr, colidx, t_rowptr, t_colidx;
     DBuf<double> vals, t_vals, sv64, stv64, dr, dc, pv, pu;
     DBuf<float> sv32, stv32;
     DBuf<int32_t> mat_m, mat_n;
     DBuf<int64_t> mat_row_off, mat_col_off;
     DBuf<double> mat_eta;
+    // SELL-32 copies: slice pointers (per matrix nslices + 1, at mat_*s_off), local
+    // indices, scaled values in both precisions; internal -> external local index
+    DBuf<int64_t> r_sptr, c_sptr, mat_rs_off, mat_cs_off;
+    DBuf<uint16_t> r_eidx, c_eidx;
+    DBuf<double> r_ev64, c_ev64;
+    DBuf<float> r_ev32, c_ev32;
+    DBuf<int32_t> r_ext, c_ext;
     std::vector<int32_t> h_mat_m, h_mat_n;
-    std::vector<int64_t> h_mat_nnz;
     // instances
     DBuf<int32_t> inst_mat;
     DBuf<int64_t> x_off, y_off;
     DBuf<double> b, c, lb, ub, bnorm, cnorm;
     DBuf<uint8_t> is_eq;
-    DBuf<double> bs, cs, ls, us, x, xa, xt, y, ya, yt;  // scaled vectors and FP64 iterates
+    // packed records and iterates, sized for FP64 and reinterpreted for FP32
+    DBuf<double> colp, rowp, x, xt, y, yt;
     bool recenter = false;
-    DBuf<double> xbar, atybar, ybar, axbar, ylb_s;      // re-centring state (per instance)
+    DBuf<double> xbar, atybar, ybar, axbar;  // re-centring state (per instance, original space)
     DBuf<InstCtrl> ictrl;
     DBuf<int32_t> active, active2, counters;  // counters[0]=head, [1]=active count
     std::vector<int32_t> h_inst_mat, order;
@@ -83,30 +112,49 @@ void batch_free(Ctx* ctx) {
 
 namespace {
 
+constexpr int kLongSlice = 128;  // entries per lane above which a slice is summed warp-cooperatively
+constexpr int kKktLanesCol = 4, kKktLanesRow = 8;
+
+// Packed per-column / per-row parameters of the scaled (and, when re-centred,
+// shifted) problem in the solve's precision.
+template <typename T>
+struct alignas(4 * sizeof(T)) ColP {
+    T c, l, u, a;  // cost, lower bound, upper bound, Halpern anchor
+};
+template <typename T>
+struct alignas(4 * sizeof(T)) RowP {
+    T b, lo, a, pad;  // rhs, lower bound of the dual (-inf on equality rows), anchor
+};
+
 struct BArgs {
     // matrices
     const int32_t *rowptr, *colidx, *t_rowptr, *t_colidx;
     const double *sv64, *stv64, *dr, *dc, *mat_eta;
-    const void *sv, *stv;  // T-typed scaled values
+    const void *sv, *stv;  // MT-typed scaled values (CSR)
     const int32_t *mat_m, *mat_n;
     const int64_t *mat_row_off, *mat_col_off;
+    // SELL-32 copies
+    const int64_t *r_sptr, *c_sptr, *mat_rs_off, *mat_cs_off;
+    const uint16_t *r_eidx, *c_eidx;
+    const void *r_ev, *c_ev;  // MT-typed
+    const int32_t *r_ext, *c_ext;
     // instances
     const int32_t* inst_mat;
     const int64_t *x_off, *y_off;
-    const double *b, *c, *lb, *ub, *bnorm, *cnorm;
+    const double *b, *c, *lb, *ub;
+    double *bnorm, *cnorm;  // written by the init kernel
     const uint8_t* is_eq;
-    double *bs, *cs, *ls, *us;  // scaled problem vectors (rewritten by re-centring)
-    double *x, *xa, *xt, *y, *ya, *yt;
+    void *colp, *rowp, *x, *xt, *y, *yt;  // MT-typed
     InstCtrl* ictrl;
     const int32_t* active;
     int32_t* counters;
     // parameters
     double eps, beta_s, beta_n, beta_a, rho;
-    // FP64 re-centring at restarts (as in the single-LP engine): per-instance centre in
-    // the original space, A xbar, A^T ybar, shifted dual bound; original FP64 values
+    // FP64 re-centring: per-instance centre in the original space, A xbar, A^T ybar;
+    // original FP64 values in both orientations
     int recenter;
     const double *vals, *t_vals;
-    double *xbar, *ybar, *axbar, *atybar, *ylb_s;
+    double *xbar, *ybar, *axbar, *atybar;
     long long max_iter;
     int K;
 };
@@ -135,20 +183,94 @@ __device__ __forceinline__ void block_sums(double (&v)[NV], double* sh /* [32*NV
     }
 }
 
-template <typename MT, int LC, int LR>
-__global__ void __launch_bounds__(512) k_batch_chunk(BArgs a, int chunk) {
+// One lane's row of a SELL-32 slice: v / ix point at the lane's first entry, the
+// next entry of the same row is 32 elements further.  Sequential sum.
+template <typename MT>
+__device__ __forceinline__ MT ell_dot(const MT* __restrict__ v, const uint16_t* __restrict__ ix, int len,
+                                      const MT* __restrict__ g) {
+    MT s = (MT)0;
+#pragma unroll 4
+    for (int q = 0; q < len; ++q) s += v[q * 32] * g[ix[q * 32]];
+    return s;
+}
+
+// The 32 rows of one slice summed by the whole warp over the CSR copy (rows
+// first .. first+cnt-1, global numbering; `off` localises the column index).
+// Lane r returns the sum of row first + r.
+template <typename MT>
+__device__ MT long_slice_dot(const MT* __restrict__ vals, const int32_t* __restrict__ ptr,
+                             const int32_t* __restrict__ idx, int64_t first, int cnt, int64_t off,
+                             const MT* __restrict__ g, int lane) {
+    MT mine = (MT)0;
+    for (int r = 0; r < cnt; ++r) {
+        MT s = (MT)0;
+        for (int e = ptr[first + r] + lane; e < ptr[first + r + 1]; e += 32) s += vals[e] * g[idx[e] - off];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if (lane == r) mine = s;
+    }
+    return mine;
+}
+
+// Re-centring, an exact change of variables in FP64: rewrite the scaled problem of
+// one instance around its centre (xbar, ybar) -- rhs dr*(b - A xbar), cost
+// dc*(c + A^T ybar), bounds (l - xbar)/dc, (u - xbar)/dc, dual lower bound -ybar/dr
+// on inequality rows -- from the original FP64 matrix, with zero anchors (the
+// iterates restart at the centre).  Called by every thread of the owning CTA.
+template <typename MT>
+__device__ void rebuild_shifted(const BArgs& a, int m, int n, int64_t ro, int64_t co, int64_t xo, int64_t yo) {
+    ColP<MT>* colp = (ColP<MT>*)a.colp;
+    RowP<MT>* rowp = (RowP<MT>*)a.rowp;
+    for (int i = threadIdx.x; i < m; i += blockDim.x) {
+        const int64_t gi = ro + i;
+        double s = 0.0;
+        for (int e = a.rowptr[gi]; e < a.rowptr[gi + 1]; ++e) s += a.vals[e] * a.xbar[xo + a.colidx[e] - co];
+        const double dri = a.dr[gi];
+        a.axbar[yo + i] = s;
+        RowP<MT> r;
+        r.b = (MT)(dri * (a.b[yo + i] - s));
+        r.lo = a.is_eq[yo + i] ? (MT)(-INFINITY) : (MT)(-a.ybar[yo + i] / dri);
+        r.a = (MT)0;
+        r.pad = (MT)0;
+        rowp[yo + i] = r;
+    }
+    for (int j = threadIdx.x; j < n; j += blockDim.x) {
+        const int64_t gj = co + j;
+        double s = 0.0;
+        for (int e = a.t_rowptr[gj]; e < a.t_rowptr[gj + 1]; ++e) s += a.t_vals[e] * a.ybar[yo + a.t_colidx[e] - ro];
+        const double dcj = a.dc[gj], xb = a.xbar[xo + j];
+        a.atybar[xo + j] = s;
+        ColP<MT> p;
+        p.c = (MT)(dcj * (a.c[xo + j] + s));
+        p.l = (MT)((a.lb[xo + j] - xb) / dcj);
+        p.u = (MT)((a.ub[xo + j] - xb) / dcj);
+        p.a = (MT)0;
+        colp[xo + j] = p;
+    }
+}
+
+template <typename MT>
+__global__ void __launch_bounds__(512, 2) k_batch_chunk(BArgs a, int chunk) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ double red[32 * 6];
     __shared__ InstCtrl sc;
     __shared__ int s_q;
-    __shared__ int s_flags[4];  // 0: done, 1: restart
+    __shared__ int s_flags[2];  // 0: done, 1: restart
     const int tid = threadIdx.x, nt = blockDim.x;
     const int lane = tid & 31, warp = tid >> 5, nwarps = nt >> 5;
     const MT* sv = (const MT*)a.sv;
     const MT* stv = (const MT*)a.stv;
-    double *bs = a.bs, *cs = a.cs, *ls = a.ls, *us = a.us;
-    double *xg = a.x, *xag = a.xa, *xtg = a.xt, *yg = a.y, *yag = a.ya, *ytg = a.yt;
+    const MT* rev = (const MT*)a.r_ev;
+    const MT* cev = (const MT*)a.c_ev;
+    ColP<MT>* colp = (ColP<MT>*)a.colp;
+    RowP<MT>* rowp = (RowP<MT>*)a.rowp;
+    MT *xg = (MT*)a.x, *xtg = (MT*)a.xt, *yg = (MT*)a.y, *ytg = (MT*)a.yt;
     const int active_count = a.counters[1];
+    const int csub = lane & (kKktLanesCol - 1), cgid = warp * (32 / kKktLanesCol) + lane / kKktLanesCol;
+    const int cgroups = nwarps * (32 / kKktLanesCol);
+    const int rsub = lane & (kKktLanesRow - 1), rgid = warp * (32 / kKktLanesRow) + lane / kKktLanesRow;
+    const int rgroups = nwarps * (32 / kKktLanesRow);
+    const MT rho = (MT)a.rho, one_rho = (MT)(1.0 + a.rho);
     while (true) {
         if (tid == 0) s_q = atomicAdd(&a.counters[0], 1);
         __syncthreads();
@@ -159,164 +281,156 @@ __global__ void __launch_bounds__(512) k_batch_chunk(BArgs a, int chunk) {
         const int m = a.mat_m[mat], n = a.mat_n[mat];
         const int64_t ro = a.mat_row_off[mat], co = a.mat_col_off[mat];
         const int64_t xo = a.x_off[inst], yo = a.y_off[inst];
+        const int64_t* rsp = a.r_sptr + a.mat_rs_off[mat];
+        const int64_t* csp = a.c_sptr + a.mat_cs_off[mat];
+        const int nrs = (m + 31) >> 5, ncs = (n + 31) >> 5;
         const double eta = a.mat_eta[mat];
-        double* ys = (double*)smem_raw;
-        MT* xhs = (MT*)(ys + ((m + 1) & ~1));
+        MT* ys = (MT*)smem_raw;
+        MT* xhs = ys + ((m + 3) & ~3);
         if (tid == 0) sc = a.ictrl[inst];
         for (int i = tid; i < m; i += nt) ys[i] = yg[yo + i];
         __syncthreads();
-        const double rho = a.rho;
-        for (int it = 0; it < chunk; ++it) {
-            const long long kk = sc.k;
-            const bool first = sc.first != 0;
-            const bool check = ((sc.total + 1) % a.K) == 0;
-            const double om = sc.omega;
-            const double tau = eta / om, sigma = eta * om;
-            const double wk = (kk + 1.0) / (kk + 2.0), wa = 1.0 / (kk + 2.0);
-            double acc[6] = {0, 0, 0, 0, 0, 0};  // rx2 (first or check), dxa2, ry2, dya2
-            // ---- primal phase: columns (gathers y from shared memory)
-            {
-                const int sub = lane & (LC - 1), per_warp = 32 / LC;
-                for (int base = warp * per_warp; base < n; base += nwarps * per_warp) {
-                    const int j = base + lane / LC;
-                    const bool valid = j < n;
-                    double s = 0.0;
-                    if (valid) {
-                        const int64_t gj = co + j;
-                        const int e1 = a.t_rowptr[gj + 1];
-                        for (int e = a.t_rowptr[gj] + sub; e < e1; e += LC) s += (double)stv[e] * ys[a.t_colidx[e] - ro];
+        long long kk = sc.k, total = sc.total;
+        bool first = sc.first != 0;
+        double om = sc.omega;
+        __syncthreads();  // every thread holds its copy before thread 0 writes sc again
+        bool done = false;
+        for (int it = 0; it < chunk && !done; ++it) {
+            const bool check = ((total + 1) % a.K) == 0;
+            const bool stats = first || check;
+            const MT tau = (MT)(eta / om), sigma = (MT)(eta * om);
+            const MT wk = (MT)((kk + 1.0) / (kk + 2.0)), wa = (MT)(1.0 / (kk + 2.0));
+            double acc[4] = {0, 0, 0, 0};  // |x - T(x)|^2 and |y - T(y)|^2 (first or check), distances to anchors
+            // ---- primal phase: one thread per column, gathers y from shared memory
+            for (int sl = warp; sl < ncs; sl += nwarps) {
+                const int j = (sl << 5) + lane;
+                const bool valid = j < n;
+                ColP<MT> p;
+                MT x0 = (MT)0;
+                if (valid) {
+                    p = colp[xo + j];
+                    x0 = xg[xo + j];
+                }
+                const int64_t p0 = csp[sl];
+                const int len = (int)((csp[sl + 1] - p0) >> 5);
+                const MT s = len <= kLongSlice
+                                 ? ell_dot<MT>(cev + p0 + lane, a.c_eidx + p0 + lane, len, ys)
+                                 : long_slice_dot<MT>(stv, a.t_rowptr, a.t_colidx, co + (sl << 5), min(32, n - (sl << 5)),
+                                                      ro, ys, lane);
+                if (valid) {
+                    const MT xt = clampT(x0 - tau * (p.c + s), p.l, p.u);
+                    xhs[j] = (MT)2 * xt - x0;
+                    xg[xo + j] = wk * (one_rho * xt - rho * x0) + wa * p.a;
+                    if (stats) {
+                        const double d = (double)x0 - (double)xt;
+                        acc[0] += d * d;
                     }
-#pragma unroll
-                    for (int o = LC / 2; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-                    if (valid && sub == 0) {
-                        const double xj = xg[xo + j];
-                        const double xt = clampT(xj - tau * (cs[xo + j] + s), ls[xo + j], us[xo + j]);
-                        xhs[j] = (MT)(2.0 * xt - xj);
-                        const double xa = xag[xo + j];
-                        xg[xo + j] = wk * ((1.0 + rho) * xt - rho * xj) + wa * xa;
-                        if (first || check) {
-                            double d = xj - xt;
-                            acc[0] += d * d;
-                        }
-                        if (check) {
-                            xtg[xo + j] = xt;
-                            double e = xt - xa;
-                            acc[1] += e * e;
-                        }
+                    if (check) {
+                        xtg[xo + j] = xt;
+                        const double e = (double)xt - (double)p.a;
+                        acc[1] += e * e;
                     }
                 }
             }
             __syncthreads();
-            // ---- dual phase: rows (gathers xh from shared memory)
-            {
-                const int sub = lane & (LR - 1), per_warp = 32 / LR;
-                for (int base = warp * per_warp; base < m; base += nwarps * per_warp) {
-                    const int i = base + lane / LR;
-                    const bool valid = i < m;
-                    double s = 0.0;
-                    if (valid) {
-                        const int64_t gi = ro + i;
-                        const int e1 = a.rowptr[gi + 1];
-                        for (int e = a.rowptr[gi] + sub; e < e1; e += LR) s += (double)sv[e] * (double)xhs[a.colidx[e] - co];
+            // ---- dual phase: one thread per row, gathers xh from shared memory
+            for (int sl = warp; sl < nrs; sl += nwarps) {
+                const int i = (sl << 5) + lane;
+                const bool valid = i < m;
+                RowP<MT> p;
+                if (valid) p = rowp[yo + i];
+                const int64_t p0 = rsp[sl];
+                const int len = (int)((rsp[sl + 1] - p0) >> 5);
+                const MT s = len <= kLongSlice
+                                 ? ell_dot<MT>(rev + p0 + lane, a.r_eidx + p0 + lane, len, xhs)
+                                 : long_slice_dot<MT>(sv, a.rowptr, a.colidx, ro + (sl << 5), min(32, m - (sl << 5)),
+                                                      co, xhs, lane);
+                if (valid) {
+                    const MT y0 = ys[i];
+                    MT yt = y0 + sigma * (s - p.b);
+                    if (yt < p.lo) yt = p.lo;  // NaN stays NaN
+                    ys[i] = wk * (one_rho * yt - rho * y0) + wa * p.a;
+                    if (stats) {
+                        const double d = (double)y0 - (double)yt;
+                        acc[2] += d * d;
                     }
-#pragma unroll
-                    for (int o = LR / 2; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-                    if (valid && sub == 0) {
-                        const double yi = ys[i];
-                        double yt = yi + sigma * (s - bs[yo + i]);
-                        if (!a.is_eq[yo + i]) {
-                            const double lbv = a.recenter ? a.ylb_s[yo + i] : 0.0;
-                            if (yt < lbv) yt = lbv;
-                        }
-                        const double ya = yag[yo + i];
-                        ys[i] = wk * ((1.0 + rho) * yt - rho * yi) + wa * ya;
-                        if (first || check) {
-                            double d = yi - yt;
-                            acc[2] += d * d;
-                        }
-                        if (check) {
-                            ytg[yo + i] = yt;
-                            double e = yt - ya;
-                            acc[3] += e * e;
-                        }
+                    if (check) {
+                        ytg[yo + i] = yt;
+                        const double e = (double)yt - (double)p.a;
+                        acc[3] += e * e;
                     }
                 }
             }
-            if (first || check) block_sums<6>(acc, red);
-            __syncthreads();
-            if (tid == 0) {
-                if (first) {
-                    sc.r0 = sqrt(om * acc[0] + acc[2] / om);
-                    sc.rprev = sc.r0;
-                    sc.first = 0;
-                }
-                sc.k += 1;
-                sc.total += 1;
-                s_flags[0] = 0;
-                s_flags[1] = 0;
-            }
-            if (!check) {
+            kk += 1;
+            total += 1;
+            if (!stats) {
                 __syncthreads();
                 continue;
             }
-            // restart residuals (thread 0 holds the block sums)
+            block_sums<4>(acc, red);
+            const bool was_first = first;
+            first = false;
+            if (!check) {  // first iteration after a (re)start: the restart reference residual
+                if (tid == 0) {
+                    sc.r0 = sqrt(om * acc[0] + acc[2] / om);
+                    sc.rprev = sc.r0;
+                }
+                __syncthreads();
+                continue;
+            }
             double r_now = 0, dxa = 0, dya = 0;
             if (tid == 0) {
                 r_now = sqrt(om * acc[0] + acc[2] / om);
+                if (was_first) {
+                    sc.r0 = r_now;
+                    sc.rprev = r_now;
+                }
                 dxa = sqrt(acc[1]);
                 dya = sqrt(acc[3]);
             }
             __syncthreads();  // xt / yt of this iteration are in global memory
-            // ---- FP64 KKT of T(z) on the original instance
-            double kk2[6] = {0, 0, 0, 0, 0, 0};  // pres2, by, dres2, pc, lam
-            {
-                const int sub = lane & (LR - 1), per_warp = 32 / LR;
-                for (int base = warp * per_warp; base < m; base += nwarps * per_warp) {
-                    const int i = base + lane / LR;
-                    const bool valid = i < m;
-                    double s = 0.0;
-                    if (valid) {
-                        const int64_t gi = ro + i;
-                        for (int e = a.rowptr[gi] + sub; e < a.rowptr[gi + 1]; e += LR)
-                            s += a.sv64[e] * xtg[xo + a.colidx[e] - co];
-                    }
+            // ---- FP64 KKT of T(z) on the original instance (CSR, sub-warp per row / column)
+            double kk2[6] = {0, 0, 0, 0, 0, 0};  // |primal residual|^2, b.y, |dual residual|^2, c.x, bound term
+            for (int base = 0; base < m; base += rgroups) {
+                const int i = base + rgid;
+                double s = 0.0;
+                if (i < m) {
+                    const int64_t gi = ro + i;
+                    for (int e = a.rowptr[gi] + rsub; e < a.rowptr[gi + 1]; e += kKktLanesRow)
+                        s += a.sv64[e] * (double)xtg[xo + a.colidx[e] - co];
+                }
 #pragma unroll
-                    for (int o = LR / 2; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-                    if (valid && sub == 0) {
-                        const double dri = a.dr[ro + i];
-                        const double ax = (a.recenter ? a.axbar[yo + i] : 0.0) + s / dri;
-                        double rp = ax - a.b[yo + i];
-                        if (!a.is_eq[yo + i]) rp = fmax(rp, 0.0);
-                        kk2[0] += rp * rp;
-                        kk2[1] += a.b[yo + i] * ((a.recenter ? a.ybar[yo + i] : 0.0) + dri * ytg[yo + i]);
-                    }
+                for (int o = kKktLanesRow / 2; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+                if (i < m && rsub == 0) {
+                    const double dri = a.dr[ro + i];
+                    const double ax = (a.recenter ? a.axbar[yo + i] : 0.0) + s / dri;
+                    double rp = ax - a.b[yo + i];
+                    if (!a.is_eq[yo + i]) rp = fmax(rp, 0.0);
+                    kk2[0] += rp * rp;
+                    kk2[1] += a.b[yo + i] * ((a.recenter ? a.ybar[yo + i] : 0.0) + dri * (double)ytg[yo + i]);
                 }
             }
-            {
-                const int sub = lane & (LC - 1), per_warp = 32 / LC;
-                for (int base = warp * per_warp; base < n; base += nwarps * per_warp) {
-                    const int j = base + lane / LC;
-                    const bool valid = j < n;
-                    double s = 0.0;
-                    if (valid) {
-                        const int64_t gj = co + j;
-                        for (int e = a.t_rowptr[gj] + sub; e < a.t_rowptr[gj + 1]; e += LC)
-                            s += a.stv64[e] * ytg[yo + a.t_colidx[e] - ro];
-                    }
+            for (int base = 0; base < n; base += cgroups) {
+                const int j = base + cgid;
+                double s = 0.0;
+                if (j < n) {
+                    const int64_t gj = co + j;
+                    for (int e = a.t_rowptr[gj] + csub; e < a.t_rowptr[gj + 1]; e += kKktLanesCol)
+                        s += a.stv64[e] * (double)ytg[yo + a.t_colidx[e] - ro];
+                }
 #pragma unroll
-                    for (int o = LC / 2; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-                    if (valid && sub == 0) {
-                        const double dcj = a.dc[co + j];
-                        const double cj = a.c[xo + j], lj = a.lb[xo + j], uj = a.ub[xo + j];
-                        const double g = cj + (a.recenter ? a.atybar[xo + j] : 0.0) + s / dcj;
-                        const bool fl = isfinite(lj), fu = isfinite(uj);
-                        const double lam = (fl && fu) ? g : (fl ? fmax(g, 0.0) : (fu ? fmin(g, 0.0) : 0.0));
-                        const double rd = g - lam;
-                        kk2[2] += rd * rd;
-                        kk2[3] += cj * ((a.recenter ? a.xbar[xo + j] : 0.0) + dcj * xtg[xo + j]);
-                        if (lam > 0.0) kk2[4] += lam * lj;
-                        else if (lam < 0.0) kk2[4] += lam * uj;
-                    }
+                for (int o = kKktLanesCol / 2; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+                if (j < n && csub == 0) {
+                    const double dcj = a.dc[co + j];
+                    const double cj = a.c[xo + j], lj = a.lb[xo + j], uj = a.ub[xo + j];
+                    const double g = cj + (a.recenter ? a.atybar[xo + j] : 0.0) + s / dcj;
+                    const bool fl = isfinite(lj), fu = isfinite(uj);
+                    const double lam = (fl && fu) ? g : (fl ? fmax(g, 0.0) : (fu ? fmin(g, 0.0) : 0.0));
+                    const double rd = g - lam;
+                    kk2[2] += rd * rd;
+                    kk2[3] += cj * ((a.recenter ? a.xbar[xo + j] : 0.0) + dcj * (double)xtg[xo + j]);
+                    if (lam > 0.0) kk2[4] += lam * lj;
+                    else if (lam < 0.0) kk2[4] += lam * uj;
                 }
             }
             block_sums<6>(kk2, red);
@@ -335,21 +449,20 @@ __global__ void __launch_bounds__(512) k_batch_chunk(BArgs a, int chunk) {
                 } else if (sc.rel_p <= a.eps && sc.rel_d <= a.eps && sc.rel_g <= a.eps) {
                     sc.done = 1;
                     sc.status = B2P_STATUS_OPTIMAL;
-                } else if (sc.total >= a.max_iter) {
+                } else if (total >= a.max_iter) {
                     sc.done = 1;
                     sc.status = B2P_STATUS_MAX_ITERATIONS;
                 }
+                s_flags[1] = 0;
                 if (!sc.done) {
                     const bool rs = (r_now <= a.beta_s * sc.r0) || (r_now <= a.beta_n * sc.r0 && r_now > sc.rprev) ||
-                                    ((double)sc.k >= a.beta_a * (double)sc.total);
+                                    ((double)kk >= a.beta_a * (double)total);
                     sc.rprev = r_now;
                     if (rs) {
                         if (dxa > 1e-10 && dya > 1e-10) {
                             const double nw = exp(0.5 * log(dya / dxa) + 0.5 * log(om));
                             if (isfinite(nw) && nw > 0.0) sc.omega = nw;
                         }
-                        sc.k = 0;
-                        sc.first = 1;
                         sc.restarts += 1;
                         s_flags[1] = 1;
                     }
@@ -357,60 +470,47 @@ __global__ void __launch_bounds__(512) k_batch_chunk(BArgs a, int chunk) {
                 s_flags[0] = sc.done;
             }
             __syncthreads();
-            if (s_flags[1] && !a.recenter) {  // restart: z <- anchor <- T(z)
-                for (int j = tid; j < n; j += nt) {
-                    const double v = xtg[xo + j];
-                    xg[xo + j] = v;
-                    xag[xo + j] = v;
-                }
-                for (int i = tid; i < m; i += nt) {
-                    const double v = ytg[yo + i];
-                    ys[i] = v;
-                    yag[yo + i] = v;
-                }
-            } else if (s_flags[1]) {
-                // restart with re-centring: the LP is rewritten around T(z) (an exact change of
-                // variables) with b - A xbar and c + A^T ybar from the FP64 original matrix
-                for (int j = tid; j < n; j += nt) {
-                    a.xbar[xo + j] += a.dc[co + j] * xtg[xo + j];
-                    xg[xo + j] = 0.0;
-                    xag[xo + j] = 0.0;
-                    xtg[xo + j] = 0.0;
-                }
-                for (int i = tid; i < m; i += nt) {
-                    a.ybar[yo + i] += a.dr[ro + i] * ytg[yo + i];
-                    ys[i] = 0.0;
-                    yag[yo + i] = 0.0;
-                    ytg[yo + i] = 0.0;
-                }
-                __syncthreads();
-                for (int i = tid; i < m; i += nt) {
-                    const int64_t gi = ro + i;
-                    double s = 0.0;
-                    for (int e = a.rowptr[gi]; e < a.rowptr[gi + 1]; ++e) s += a.vals[e] * a.xbar[xo + a.colidx[e] - co];
-                    const double dri = a.dr[gi];
-                    a.axbar[yo + i] = s;
-                    bs[yo + i] = dri * (a.b[yo + i] - s);
-                    a.ylb_s[yo + i] = -a.ybar[yo + i] / dri;
-                }
-                for (int j = tid; j < n; j += nt) {
-                    const int64_t gj = co + j;
-                    double s = 0.0;
-                    for (int e = a.t_rowptr[gj]; e < a.t_rowptr[gj + 1]; ++e)
-                        s += a.t_vals[e] * a.ybar[yo + a.t_colidx[e] - ro];
-                    const double dcj = a.dc[gj];
-                    a.atybar[xo + j] = s;
-                    cs[xo + j] = dcj * (a.c[xo + j] + s);
-                    ls[xo + j] = (a.lb[xo + j] - a.xbar[xo + j]) / dcj;
-                    us[xo + j] = (a.ub[xo + j] - a.xbar[xo + j]) / dcj;
+            done = s_flags[0] != 0;
+            om = sc.omega;
+            if (s_flags[1]) {
+                kk = 0;
+                first = true;
+                if (!a.recenter) {  // restart: z <- anchor <- T(z)
+                    for (int j = tid; j < n; j += nt) {
+                        const MT v = xtg[xo + j];
+                        xg[xo + j] = v;
+                        colp[xo + j].a = v;
+                    }
+                    for (int i = tid; i < m; i += nt) {
+                        const MT v = ytg[yo + i];
+                        ys[i] = v;
+                        rowp[yo + i].a = v;
+                    }
+                } else {  // restart at T(z) as the new FP64 centre
+                    for (int j = tid; j < n; j += nt) {
+                        a.xbar[xo + j] += a.dc[co + j] * (double)xtg[xo + j];
+                        xg[xo + j] = (MT)0;
+                        xtg[xo + j] = (MT)0;
+                    }
+                    for (int i = tid; i < m; i += nt) {
+                        a.ybar[yo + i] += a.dr[ro + i] * (double)ytg[yo + i];
+                        ys[i] = (MT)0;
+                        ytg[yo + i] = (MT)0;
+                    }
+                    __syncthreads();
+                    rebuild_shifted<MT>(a, m, n, ro, co, xo, yo);
                 }
             }
             __syncthreads();
-            if (s_flags[0]) break;
         }
         // store the dual iterate and the control block
         for (int i = tid; i < m; i += nt) yg[yo + i] = ys[i];
-        if (tid == 0) a.ictrl[inst] = sc;
+        if (tid == 0) {
+            sc.k = kk;
+            sc.total = total;
+            sc.first = first ? 1 : 0;
+            a.ictrl[inst] = sc;
+        }
         __syncthreads();
     }
 }
@@ -438,10 +538,6 @@ __global__ void k_batch_compact(const InstCtrl* __restrict__ ictrl, const int32_
         counters[1] = base;
         counters[0] = 0;
     }
-}
-
-__global__ void k_copy_i32(int n, const int32_t* __restrict__ a, int32_t* __restrict__ b) {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) b[i] = a[i];
 }
 
 // ------------------------------------------------------------------ setup kernels (CTA per matrix, FP64)
@@ -577,101 +673,177 @@ __global__ void k_batch_power(int nmat, const int32_t* __restrict__ mat_m, const
     }
 }
 
-// per-instance scaled vectors, norms, initial point and control block (CTA per instance)
-template <typename T>
-__global__ void k_batch_init(int count, const int32_t* __restrict__ inst_mat, const int32_t* __restrict__ mat_m,
-                             const int32_t* __restrict__ mat_n, const int64_t* __restrict__ row_off,
-                             const int64_t* __restrict__ col_off, const int64_t* __restrict__ x_off,
-                             const int64_t* __restrict__ y_off, const double* __restrict__ dr,
-                             const double* __restrict__ dc, const double* __restrict__ b, const double* __restrict__ c,
-                             const double* __restrict__ lb, const double* __restrict__ ub,
-                             const uint8_t* __restrict__ is_eq, const double* __restrict__ x0,
-                             const double* __restrict__ y0, const double* __restrict__ omega0, T* bs, T* cs, T* ls,
-                             T* us, T* x, T* xa, T* xt, T* y, T* ya, T* yt, double* bnorm, double* cnorm,
-                             InstCtrl* ictrl) {
-    __shared__ double red[32 * 4];
+// SELL-32 copy of one orientation, CTA per matrix: every lane slot of every slice
+// (rows past the matrix end and entries past a row's end are zero padding with
+// local index 0).  ptr / idx / v64 / v32 are the CSR of that orientation in
+// global numbering; `other_off` localises its indices.
+__global__ void k_fill_ell(int nmat, const int32_t* __restrict__ dim, const int64_t* __restrict__ off,
+                           const int64_t* __restrict__ other_off, const int64_t* __restrict__ s_off,
+                           const int64_t* __restrict__ sptr, const int32_t* __restrict__ ptr,
+                           const int32_t* __restrict__ idx, const double* __restrict__ v64,
+                           const float* __restrict__ v32, uint16_t* __restrict__ eidx, double* __restrict__ ev64,
+                           float* __restrict__ ev32) {
+    for (int k = blockIdx.x; k < nmat; k += gridDim.x) {
+        const int d = dim[k];
+        const int padded = (d + 31) & ~31;
+        const int64_t base = off[k], ob = other_off[k];
+        const int64_t* sp = sptr + s_off[k];
+        for (int li = threadIdx.x; li < padded; li += blockDim.x) {
+            const int s = li >> 5, lane = li & 31;
+            const int64_t p0 = sp[s];
+            const int len = (int)((sp[s + 1] - p0) >> 5);
+            int e = 0, e1 = 0;
+            if (li < d) {
+                e = ptr[base + li];
+                e1 = ptr[base + li + 1];
+            }
+            for (int q = 0; q < len; ++q) {
+                const int64_t pos = p0 + 32 * (int64_t)q + lane;
+                if (e + q < e1) {
+                    eidx[pos] = (uint16_t)(idx[e + q] - ob);
+                    ev64[pos] = v64[e + q];
+                    ev32[pos] = v32[e + q];
+                } else {
+                    eidx[pos] = 0;
+                    ev64[pos] = 0.0;
+                    ev32[pos] = 0.0f;
+                }
+            }
+        }
+    }
+}
+
+// Per-instance b, c, l, u, row kinds from external to internal order (CTA per instance).
+__global__ void k_permute_inst(int count, const int32_t* __restrict__ inst_mat, const int32_t* __restrict__ mat_m,
+                               const int32_t* __restrict__ mat_n, const int64_t* __restrict__ row_off,
+                               const int64_t* __restrict__ col_off, const int64_t* __restrict__ x_off,
+                               const int64_t* __restrict__ y_off, const int32_t* __restrict__ r_ext,
+                               const int32_t* __restrict__ c_ext, const double* __restrict__ sb,
+                               const double* __restrict__ sc, const double* __restrict__ sl,
+                               const double* __restrict__ su, const uint8_t* __restrict__ seq, double* __restrict__ b,
+                               double* __restrict__ c, double* __restrict__ lb, double* __restrict__ ub,
+                               uint8_t* __restrict__ is_eq) {
     for (int inst = blockIdx.x; inst < count; inst += gridDim.x) {
         const int k = inst_mat[inst];
         const int m = mat_m[k], n = mat_n[k];
         const int64_t ro = row_off[k], co = col_off[k], xo = x_off[inst], yo = y_off[inst];
-        double acc[4] = {0, 0, 0, 0};  // ||b||^2, ||c||^2, ||b_s||^2, ||c_s||^2
         for (int j = threadIdx.x; j < n; j += blockDim.x) {
-            const double d = dc[co + j];
-            const double cj = c[xo + j], csj = cj * d;
-            const T l = (T)(lb[xo + j] / d), u = (T)(ub[xo + j] / d);
-            cs[xo + j] = (T)csj;
-            ls[xo + j] = l;
-            us[xo + j] = u;
-            T v = x0 ? (T)(x0[xo + j] / d) : (T)0;
-            v = clampT(v, l, u);
-            x[xo + j] = v;
-            xa[xo + j] = v;
-            xt[xo + j] = v;
-            acc[1] += cj * cj;
-            acc[3] += csj * csj;
+            const int64_t src = xo + c_ext[co + j];
+            c[xo + j] = sc[src];
+            lb[xo + j] = sl[src];
+            ub[xo + j] = su[src];
         }
         for (int i = threadIdx.x; i < m; i += blockDim.x) {
-            const double d = dr[ro + i];
-            const double bi = b[yo + i], bsi = bi * d;
-            bs[yo + i] = (T)bsi;
-            T v = y0 ? (T)(y0[yo + i] / d) : (T)0;
-            if (!is_eq[yo + i] && v < (T)0) v = (T)0;
-            y[yo + i] = v;
-            ya[yo + i] = v;
-            yt[yo + i] = v;
+            const int64_t src = yo + r_ext[ro + i];
+            b[yo + i] = sb[src];
+            is_eq[yo + i] = seq[src];
+        }
+    }
+}
+
+// Per-instance norms, initial point, packed records and control block (CTA per
+// instance).  Warm starts arrive in external order.  With re-centring the initial
+// point (warm start, else the bound projection of 0) becomes the first FP64
+// centre and the iterates start at 0.
+template <typename MT>
+__global__ void k_batch_init(BArgs a, int count, const double* __restrict__ x0, const double* __restrict__ y0,
+                             const double* __restrict__ omega0) {
+    __shared__ double red[32 * 4];
+    ColP<MT>* colp = (ColP<MT>*)a.colp;
+    RowP<MT>* rowp = (RowP<MT>*)a.rowp;
+    MT *xg = (MT*)a.x, *xtg = (MT*)a.xt, *yg = (MT*)a.y, *ytg = (MT*)a.yt;
+    for (int inst = blockIdx.x; inst < count; inst += gridDim.x) {
+        const int k = a.inst_mat[inst];
+        const int m = a.mat_m[k], n = a.mat_n[k];
+        const int64_t ro = a.mat_row_off[k], co = a.mat_col_off[k], xo = a.x_off[inst], yo = a.y_off[inst];
+        double acc[4] = {0, 0, 0, 0};  // ||b||^2, ||c||^2, ||b_s||^2, ||c_s||^2
+        for (int j = threadIdx.x; j < n; j += blockDim.x) {
+            const double d = a.dc[co + j];
+            const double cj = a.c[xo + j], lj = a.lb[xo + j], uj = a.ub[xo + j];
+            const double v = clampT(x0 ? x0[xo + a.c_ext[co + j]] : 0.0, lj, uj);
+            if (a.recenter) {
+                a.xbar[xo + j] = v;
+                xg[xo + j] = (MT)0;
+                xtg[xo + j] = (MT)0;
+            } else {
+                const MT vs = (MT)(v / d);
+                xg[xo + j] = vs;
+                xtg[xo + j] = vs;
+                ColP<MT> p;
+                p.c = (MT)(cj * d);
+                p.l = (MT)(lj / d);
+                p.u = (MT)(uj / d);
+                p.a = vs;
+                colp[xo + j] = p;
+            }
+            acc[1] += cj * cj;
+            acc[3] += (cj * d) * (cj * d);
+        }
+        for (int i = threadIdx.x; i < m; i += blockDim.x) {
+            const double d = a.dr[ro + i];
+            const double bi = a.b[yo + i];
+            const bool eq = a.is_eq[yo + i] != 0;
+            double v = y0 ? y0[yo + a.r_ext[ro + i]] : 0.0;
+            if (!eq && v < 0.0) v = 0.0;
+            if (a.recenter) {
+                a.ybar[yo + i] = v;
+                yg[yo + i] = (MT)0;
+                ytg[yo + i] = (MT)0;
+            } else {
+                const MT vs = (MT)(v / d);
+                yg[yo + i] = vs;
+                ytg[yo + i] = vs;
+                RowP<MT> r;
+                r.b = (MT)(bi * d);
+                r.lo = eq ? (MT)(-INFINITY) : (MT)0;
+                r.a = vs;
+                r.pad = (MT)0;
+                rowp[yo + i] = r;
+            }
             acc[0] += bi * bi;
-            acc[2] += bsi * bsi;
+            acc[2] += (bi * d) * (bi * d);
         }
         block_sums<4>(acc, red);
         if (threadIdx.x == 0) {
-            bnorm[inst] = sqrt(acc[0]);
-            cnorm[inst] = sqrt(acc[1]);
+            a.bnorm[inst] = sqrt(acc[0]);
+            a.cnorm[inst] = sqrt(acc[1]);
             const double bn = sqrt(acc[2]), cn = sqrt(acc[3]);
             InstCtrl s;
             memset(&s, 0, sizeof(s));
             s.omega = (omega0 && omega0[inst] > 0.0) ? omega0[inst] : ((bn > 1e-10 && cn > 1e-10) ? cn / bn : 1.0);
             s.first = 1;
             s.status = B2P_STATUS_MAX_ITERATIONS;
-            ictrl[inst] = s;
+            a.ictrl[inst] = s;
+        }
+        if (a.recenter) {
+            __syncthreads();  // the centre of this instance is complete
+            rebuild_shifted<MT>(a, m, n, ro, co, xo, yo);
         }
         __syncthreads();
     }
 }
 
+// Answers in the original space and external order: x = xbar + dc * xt, y = ybar + dr * yt.
 template <typename T>
-__global__ void k_batch_unscale(int count, const int32_t* __restrict__ inst_mat, const int32_t* __restrict__ mat_m,
-                                const int32_t* __restrict__ mat_n, const int64_t* __restrict__ row_off,
-                                const int64_t* __restrict__ col_off, const int64_t* __restrict__ x_off,
-                                const int64_t* __restrict__ y_off, const double* __restrict__ dr,
-                                const double* __restrict__ dc, const T* __restrict__ xt, const T* __restrict__ yt,
-                                const double* __restrict__ xbar, const double* __restrict__ ybar,
+__global__ void k_batch_unscale(BArgs a, int count, const double* __restrict__ xbar, const double* __restrict__ ybar,
                                 double* __restrict__ xo_, double* __restrict__ yo_) {
+    const T* xt = (const T*)a.xt;
+    const T* yt = (const T*)a.yt;
     for (int inst = blockIdx.x; inst < count; inst += gridDim.x) {
-        const int k = inst_mat[inst];
-        const int m = mat_m[k], n = mat_n[k];
-        const int64_t ro = row_off[k], co = col_off[k], xo = x_off[inst], yo = y_off[inst];
+        const int k = a.inst_mat[inst];
+        const int m = a.mat_m[k], n = a.mat_n[k];
+        const int64_t ro = a.mat_row_off[k], co = a.mat_col_off[k], xo = a.x_off[inst], yo = a.y_off[inst];
         for (int j = threadIdx.x; j < n; j += blockDim.x)
-            xo_[xo + j] = (xbar ? xbar[xo + j] : 0.0) + dc[co + j] * (double)xt[xo + j];
+            xo_[xo + a.c_ext[co + j]] = (xbar ? xbar[xo + j] : 0.0) + a.dc[co + j] * (double)xt[xo + j];
         for (int i = threadIdx.x; i < m; i += blockDim.x)
-            yo_[yo + i] = (ybar ? ybar[yo + i] : 0.0) + dr[ro + i] * (double)yt[yo + i];
+            yo_[yo + a.r_ext[ro + i]] = (ybar ? ybar[yo + i] : 0.0) + a.dr[ro + i] * (double)yt[yo + i];
     }
 }
 
 // ------------------------------------------------------------------ host side
 struct TuneCfg {
-    int lc, lr, threads, chunk;
+    int threads, chunk;
 };
-
-template <typename T>
-using ChunkFn = void (*)(BArgs, int);
-
-template <typename T>
-ChunkFn<T> chunk_kernel(int lc, int lr) {
-#define SEL(C_, R_) if (lc == C_ && lr == R_) return k_batch_chunk<T, C_, R_>;
-    SEL(4, 8) SEL(4, 16) SEL(4, 32) SEL(8, 8) SEL(8, 16) SEL(8, 32) SEL(2, 8) SEL(2, 16) SEL(2, 32)
-#undef SEL
-    return k_batch_chunk<T, 4, 16>;
-}
 
 std::string cache_path() {
     const char* p = std::getenv("B2P_AUTOTUNE_CACHE");
@@ -681,25 +853,29 @@ std::string cache_path() {
 }
 
 std::string batch_key(BatchWork* w, int precision) {
-    // signature: precision, size classes of the batch
+    // signature: kernel version, precision, size classes of the batch
     double mean_m = (double)w->inst_m / w->count, mean_n = (double)w->inst_n / w->count;
     double nnz_col = (double)w->nnz / std::max<int64_t>(w->tot_n, 1);
     std::ostringstream os;
-    os << "p" << precision << "_c" << (int)std::log2(std::max(1, w->count)) << "_m" << (int)std::log2(mean_m + 1)
-       << "_n" << (int)std::log2(mean_n + 1) << "_k" << (int)std::lround(nnz_col) << "_M" << w->max_m << "_N" << w->max_n
-       << "_shared" << (w->nmat == 1 && w->count > 1);
+    os << "batch3_p" << precision << "_c" << (int)std::log2(std::max(1, w->count)) << "_m"
+       << (int)std::log2(mean_m + 1) << "_n" << (int)std::log2(mean_n + 1) << "_k" << (int)std::lround(nnz_col) << "_M"
+       << w->max_m << "_N" << w->max_n << "_shared" << (w->nmat == 1 && w->count > 1);
     return os.str();
 }
 
 bool cache_lookup(const std::string& key, TuneCfg* out) {
     std::ifstream f(cache_path());
-    std::string k;
-    TuneCfg c;
-    while (f >> k >> c.lc >> c.lr >> c.threads >> c.chunk)
-        if (k == key) {
+    std::string line;
+    while (std::getline(f, line)) {
+        std::istringstream is(line);
+        std::string k;
+        TuneCfg c;
+        if (!(is >> k) || k != key) continue;
+        if (is >> c.threads >> c.chunk) {
             *out = c;
             return true;
         }
+    }
     return false;
 }
 
@@ -711,10 +887,12 @@ void cache_store(const std::string& key, const TuneCfg& c) {
         if (std::system(cmd.c_str()) != 0) return;
     }
     std::ofstream f(p, std::ios::app);
-    f << key << " " << c.lc << " " << c.lr << " " << c.threads << " " << c.chunk << "\n";
+    f << key << " " << c.threads << " " << c.chunk << "\n";
 }
 
-BArgs make_args(BatchWork* w, const b2p_params* p, const void* sv, const void* stv, const int32_t* active) {
+template <typename MT>
+BArgs make_args(BatchWork* w, const b2p_params* p, const int32_t* active) {
+    const bool f64 = sizeof(MT) == 8;
     BArgs a;
     a.rowptr = w->rowptr.p;
     a.colidx = w->colidx.p;
@@ -725,12 +903,22 @@ BArgs make_args(BatchWork* w, const b2p_params* p, const void* sv, const void* s
     a.dr = w->dr.p;
     a.dc = w->dc.p;
     a.mat_eta = w->mat_eta.p;
-    a.sv = sv;
-    a.stv = stv;
+    a.sv = f64 ? (const void*)w->sv64.p : (const void*)w->sv32.p;
+    a.stv = f64 ? (const void*)w->stv64.p : (const void*)w->stv32.p;
     a.mat_m = w->mat_m.p;
     a.mat_n = w->mat_n.p;
     a.mat_row_off = w->mat_row_off.p;
     a.mat_col_off = w->mat_col_off.p;
+    a.r_sptr = w->r_sptr.p;
+    a.c_sptr = w->c_sptr.p;
+    a.mat_rs_off = w->mat_rs_off.p;
+    a.mat_cs_off = w->mat_cs_off.p;
+    a.r_eidx = w->r_eidx.p;
+    a.c_eidx = w->c_eidx.p;
+    a.r_ev = f64 ? (const void*)w->r_ev64.p : (const void*)w->r_ev32.p;
+    a.c_ev = f64 ? (const void*)w->c_ev64.p : (const void*)w->c_ev32.p;
+    a.r_ext = w->r_ext.p;
+    a.c_ext = w->c_ext.p;
     a.inst_mat = w->inst_mat.p;
     a.x_off = w->x_off.p;
     a.y_off = w->y_off.p;
@@ -741,15 +929,11 @@ BArgs make_args(BatchWork* w, const b2p_params* p, const void* sv, const void* s
     a.bnorm = w->bnorm.p;
     a.cnorm = w->cnorm.p;
     a.is_eq = w->is_eq.p;
-    a.bs = w->bs.p;
-    a.cs = w->cs.p;
-    a.ls = w->ls.p;
-    a.us = w->us.p;
+    a.colp = w->colp.p;
+    a.rowp = w->rowp.p;
     a.x = w->x.p;
-    a.xa = w->xa.p;
     a.xt = w->xt.p;
     a.y = w->y.p;
-    a.ya = w->ya.p;
     a.yt = w->yt.p;
     a.ictrl = w->ictrl.p;
     a.active = active;
@@ -768,34 +952,28 @@ BArgs make_args(BatchWork* w, const b2p_params* p, const void* sv, const void* s
     a.ybar = w->ybar.p;
     a.axbar = w->axbar.p;
     a.atybar = w->atybar.p;
-    a.ylb_s = w->ylb_s.p;
     return a;
 }
 
-// dynamic shared memory of one CTA: y (FP64) and xh (MT) of the largest instance
+// dynamic shared memory of one CTA: y and xh (MT) of the largest instance
 size_t smem_bytes(BatchWork* w, size_t mt_size) {
-    return 8 * (size_t)((w->max_m + 1) & ~1) + mt_size * (size_t)w->max_n + 16;
+    return mt_size * ((size_t)((w->max_m + 3) & ~3) + (size_t)w->max_n) + 16;
 }
 
-int init_instances(Ctx* ctx, BatchWork* w, const double* x0_dev, const double* y0_dev, const double* om_dev) {
+template <typename MT>
+int init_instances(Ctx* ctx, BatchWork* w, const b2p_params* p, const double* x0_dev, const double* y0_dev,
+                   const double* om_dev) {
     int grid = std::min(w->count, ctx->sm_count * 8);
-    k_batch_init<double><<<grid, 256, 0, ctx->stream>>>(
-        w->count, w->inst_mat.p, w->mat_m.p, w->mat_n.p, w->mat_row_off.p, w->mat_col_off.p, w->x_off.p, w->y_off.p,
-        w->dr.p, w->dc.p, w->b.p, w->c.p, w->lb.p, w->ub.p, w->is_eq.p, x0_dev, y0_dev, om_dev, w->bs.p, w->cs.p,
-        w->ls.p, w->us.p, w->x.p, w->xa.p, w->xt.p, w->y.p, w->ya.p, w->yt.p, w->bnorm.p, w->cnorm.p, w->ictrl.p);
+    BArgs a = make_args<MT>(w, p, w->active.p);
+    k_batch_init<MT><<<grid, 256, 0, ctx->stream>>>(a, w->count, x0_dev, y0_dev, om_dev);
     B2P_LAUNCH(ctx);
     ctx->launches += 1;
     return B2P_OK;
 }
 
-template <typename MT>
-const void* vals_of(BatchWork* w, bool transposed) {
-    if (sizeof(MT) == 8) return transposed ? (const void*)w->stv64.p : (const void*)w->sv64.p;
-    return transposed ? (const void*)w->stv32.p : (const void*)w->sv32.p;
-}
-
-// Times each candidate on a size-stratified sample of the batch (no termination,
-// fixed iteration count); instance state is re-initialised afterwards by the caller.
+// Times each block size on a size-stratified sample of the batch (no termination,
+// fixed iteration count, no re-centring); instance state is re-initialised
+// afterwards by the caller.
 template <typename MT>
 int autotune(Ctx* ctx, BatchWork* w, const b2p_params* p, TuneCfg* best) {
     std::string key = batch_key(w, sizeof(MT) == 8 ? 0 : 1);
@@ -811,27 +989,23 @@ int autotune(Ctx* ctx, BatchWork* w, const b2p_params* p, TuneCfg* best) {
     tp.max_iterations = 1LL << 40;
     tp.eps_rel_kkt = 0.0;  // never terminates inside the trial
     const int trial_iters = 128;
-    std::vector<TuneCfg> cands;
-    for (int lc : {2, 4, 8})
-        for (int lr : {8, 16, 32})
-            for (int th : {128, 256, 512}) cands.push_back({lc, lr, th, 2048});
     float best_ms = 1e30f;
-    *best = {4, 16, 256, 2048};
+    *best = {256, 2048};
     size_t sm = smem_bytes(w, sizeof(MT));
-    for (const TuneCfg& c : cands) {
-        int st = init_instances(ctx, w, nullptr, nullptr, nullptr);
+    for (int th : {128, 256, 512}) {
+        int st = init_instances<MT>(ctx, w, &tp, nullptr, nullptr, nullptr);
         if (st) return st;
         int32_t cnt[2] = {0, sample};
         B2P_CUDA(ctx, cudaMemcpyAsync(w->counters.p, cnt, sizeof(cnt), cudaMemcpyHostToDevice, s));
-        BArgs a = make_args(w, &tp, vals_of<MT>(w, false), vals_of<MT>(w, true), dids.p);
-        ChunkFn<MT> fn = chunk_kernel<MT>(c.lc, c.lr);
+        BArgs a = make_args<MT>(w, &tp, dids.p);
+        auto fn = k_batch_chunk<MT>;
         B2P_CUDA(ctx, cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
         int per_sm = 0;
-        B2P_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, c.threads, sm));
+        B2P_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, th, sm));
         if (per_sm < 1) continue;
         int grid = std::min(sample, ctx->sm_count * per_sm);
         cudaEventRecord(ctx->ev0, s);
-        fn<<<grid, c.threads, sm, s>>>(a, trial_iters);
+        fn<<<grid, th, sm, s>>>(a, trial_iters);
         cudaEventRecord(ctx->ev1, s);
         B2P_LAUNCH(ctx);
         B2P_CUDA(ctx, cudaEventSynchronize(ctx->ev1));
@@ -840,7 +1014,7 @@ int autotune(Ctx* ctx, BatchWork* w, const b2p_params* p, TuneCfg* best) {
         cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
         if (ms < best_ms) {
             best_ms = ms;
-            *best = c;
+            *best = {th, 2048};
         }
     }
     cache_store(key, *best);
@@ -854,13 +1028,9 @@ int batch_run(Ctx* ctx, BatchWork* w, const b2p_params* p, const double* x0, con
     cudaStream_t s = ctx->stream;
     double t_start = now_ms();
     const int64_t IN = w->inst_n, IM = w->inst_m;
-    w->recenter = false;  // autotune trials run without re-centring (its buffers are set up below)
-    // lanes per column / row, threads per CTA, chunk length: explicit, cached or tuned now
-    TuneCfg cfg = {4, 16, 256, 2048};
-    if (p->lanes_per_row > 0) {
-        cfg.lc = std::min(8, std::max(2, p->lanes_per_row / 4));
-        cfg.lr = p->lanes_per_row < 8 ? 8 : std::min(32, p->lanes_per_row);
-    } else {
+    w->recenter = false;  // autotune trials run without re-centring
+    TuneCfg cfg = {256, 2048};
+    {
         int st = autotune<MT>(ctx, w, p, &cfg);
         if (st) return st;
     }
@@ -878,26 +1048,20 @@ int batch_run(Ctx* ctx, BatchWork* w, const b2p_params* p, const double* x0, con
         B2P_CUDA(ctx, dom.reserve(w->count));
         B2P_CUDA(ctx, cudaMemcpyAsync(dom.p, omega0, sizeof(double) * w->count, cudaMemcpyHostToDevice, s));
     }
-    int st = init_instances(ctx, w, x0 ? dx0.p : nullptr, y0 ? dy0.p : nullptr, omega0 ? dom.p : nullptr);
-    if (st) return st;
     // re-centring: on by default for the mixed engine (refinement_rounds < 0), forced by > 0
     w->recenter = p->refinement_rounds > 0 || (p->refinement_rounds < 0 && sizeof(MT) == 4);
     if (w->recenter) {
-        for (auto* b : {&w->xbar, &w->atybar}) {
-            B2P_CUDA(ctx, b->reserve(IN));
-            B2P_CUDA(ctx, cudaMemsetAsync(b->p, 0, sizeof(double) * IN, s));
-        }
-        for (auto* b : {&w->ybar, &w->axbar, &w->ylb_s}) {
-            B2P_CUDA(ctx, b->reserve(IM));
-            B2P_CUDA(ctx, cudaMemsetAsync(b->p, 0, sizeof(double) * IM, s));
-        }
+        for (auto* b : {&w->xbar, &w->atybar}) B2P_CUDA(ctx, b->reserve(IN));
+        for (auto* b : {&w->ybar, &w->axbar}) B2P_CUDA(ctx, b->reserve(IM));
     }
+    int st = init_instances<MT>(ctx, w, p, x0 ? dx0.p : nullptr, y0 ? dy0.p : nullptr, omega0 ? dom.p : nullptr);
+    if (st) return st;
     // active list = all instances, longest first
     B2P_CUDA(ctx, cudaMemcpyAsync(w->active.p, w->order.data(), sizeof(int32_t) * w->count, cudaMemcpyHostToDevice, s));
     int32_t cnt[2] = {0, w->count};
     B2P_CUDA(ctx, cudaMemcpyAsync(w->counters.p, cnt, sizeof(cnt), cudaMemcpyHostToDevice, s));
     size_t sm = smem_bytes(w, sizeof(MT));
-    ChunkFn<MT> fn = chunk_kernel<MT>(cfg.lc, cfg.lr);
+    auto fn = k_batch_chunk<MT>;
     B2P_CUDA(ctx, cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
     int per_sm = 0;
     B2P_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, cfg.threads, sm));
@@ -906,8 +1070,8 @@ int batch_run(Ctx* ctx, BatchWork* w, const b2p_params* p, const double* x0, con
         return B2P_INVALID_ARGUMENT;
     }
     const int grid = ctx->sm_count * per_sm;
-    BArgs a1 = make_args(w, p, vals_of<MT>(w, false), vals_of<MT>(w, true), w->active.p);
-    BArgs a2 = make_args(w, p, vals_of<MT>(w, false), vals_of<MT>(w, true), w->active2.p);
+    BArgs a1 = make_args<MT>(w, p, w->active.p);
+    BArgs a2 = make_args<MT>(w, p, w->active2.p);
     // one graph = two chunk launches with compaction (ping-pong active lists)
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
@@ -960,10 +1124,8 @@ int batch_run(Ctx* ctx, BatchWork* w, const b2p_params* p, const double* x0, con
         DBuf<double> ox, oy;
         B2P_CUDA(ctx, ox.reserve(IN));
         B2P_CUDA(ctx, oy.reserve(IM));
-        k_batch_unscale<double><<<std::min(w->count, ctx->sm_count * 8), 256, 0, s>>>(
-            w->count, w->inst_mat.p, w->mat_m.p, w->mat_n.p, w->mat_row_off.p, w->mat_col_off.p, w->x_off.p, w->y_off.p,
-            w->dr.p, w->dc.p, w->xt.p, w->yt.p, w->recenter ? w->xbar.p : nullptr, w->recenter ? w->ybar.p : nullptr,
-            ox.p, oy.p);
+        k_batch_unscale<MT><<<std::min(w->count, ctx->sm_count * 8), 256, 0, s>>>(
+            a1, w->count, w->recenter ? w->xbar.p : nullptr, w->recenter ? w->ybar.p : nullptr, ox.p, oy.p);
         B2P_LAUNCH(ctx);
         ctx->launches += 1;
         if (x_out) B2P_CUDA(ctx, cudaMemcpyAsync(x_out, ox.p, sizeof(double) * IN, cudaMemcpyDeviceToHost, s));
@@ -991,8 +1153,8 @@ int batch_run(Ctx* ctx, BatchWork* w, const b2p_params* p, const double* x0, con
         sum->restarts = maxit;      // longest instance
         sum->rel_kkt = worst;
         sum->kernel_time_ms = kms;
-        sum->primal_weight = cfg.lc * 100 + cfg.lr;               // tuned lanes: column*100 + row
-        sum->step_size = cfg.threads * 100000.0 + cfg.chunk;      // tuned threads*1e5 + chunk
+        sum->primal_weight = 0.0;
+        sum->step_size = cfg.threads * 100000.0 + cfg.chunk;  // tuned block size * 1e5 + chunk length
     }
     return B2P_OK;
 }
@@ -1021,12 +1183,15 @@ int b2p_batch_upload(void* p, int nmat, const int32_t* mat_m, const int32_t* mat
     ctx->bw = w;
     w->nmat = nmat;
     w->count = count;
-    // global CSR (block diagonal), host side
     std::vector<int64_t> row_off(nmat), col_off(nmat);
     int64_t tm = 0, tn = 0;
     for (int k = 0; k < nmat; ++k) {
         if (mat_m[k] <= 0 || mat_n[k] <= 0) {
             ctx->err = "b2p_batch_upload: empty matrix";
+            return B2P_INVALID_ARGUMENT;
+        }
+        if (mat_m[k] > 65535 || mat_n[k] > 65535) {
+            ctx->err = "b2p_batch_upload: a batched instance has at most 65535 rows and columns";
             return B2P_INVALID_ARGUMENT;
         }
         row_off[k] = tm;
@@ -1044,9 +1209,17 @@ int b2p_batch_upload(void* p, int nmat, const int32_t* mat_m, const int32_t* mat
     w->tot_m = tm;
     w->tot_n = tn;
     w->nnz = nnz;
-    std::vector<int32_t> grp(tm + 1), gci(nnz);
-    int64_t rp_base = 0;
+    // validate, then renumber rows and columns of each matrix by decreasing length
+    // (stable) and build the internal CSR (global indices) and the SELL-32 slice
+    // pointers of both orientations
+    std::vector<int32_t> grp(tm + 1), gci(nnz), r_ext(tm), c_ext(tn);
+    std::vector<double> gval(nnz);
+    std::vector<int64_t> rs_off(nmat), cs_off(nmat), r_sptr, c_sptr;
+    r_sptr.reserve(tm / 32 + 2 * nmat);
+    c_sptr.reserve(tn / 32 + 2 * nmat);
+    int64_t rp_base = 0, r_pad = 0, c_pad = 0, pos = 0;
     grp[0] = 0;
+    std::vector<int32_t> rlen, clen, rord, cord, cinv;
     for (int k = 0; k < nmat; ++k) {
         const int32_t* rp = rowptr + rp_base;
         const int m = mat_m[k], n = mat_n[k];
@@ -1055,12 +1228,13 @@ int b2p_batch_upload(void* p, int nmat, const int32_t* mat_m, const int32_t* mat
             ctx->err = "b2p_batch_upload: matrix " + std::to_string(k) + " row pointers do not match its nnz";
             return B2P_INVALID_ARGUMENT;
         }
+        rlen.assign(m, 0);
+        clen.assign(n, 0);
         for (int i = 0; i < m; ++i) {
             if (rp[i + 1] < rp[i]) {
                 ctx->err = "b2p_batch_upload: decreasing row pointer";
                 return B2P_INVALID_ARGUMENT;
             }
-            grp[row_off[k] + i + 1] = (int32_t)(e0 + rp[i + 1]);
             int prev = -1;
             for (int e = rp[i]; e < rp[i + 1]; ++e) {
                 int cidx = colidx[e0 + e];
@@ -1070,9 +1244,44 @@ int b2p_batch_upload(void* p, int nmat, const int32_t* mat_m, const int32_t* mat
                     return B2P_INVALID_ARGUMENT;
                 }
                 prev = cidx;
-                gci[e0 + e] = (int32_t)(cidx + col_off[k]);
+                clen[cidx]++;
             }
+            rlen[i] = rp[i + 1] - rp[i];
         }
+        rord.resize(m);
+        cord.resize(n);
+        std::iota(rord.begin(), rord.end(), 0);
+        std::iota(cord.begin(), cord.end(), 0);
+        std::stable_sort(rord.begin(), rord.end(), [&](int x, int y) { return rlen[x] > rlen[y]; });
+        std::stable_sort(cord.begin(), cord.end(), [&](int x, int y) { return clen[x] > clen[y]; });
+        cinv.resize(n);
+        for (int j = 0; j < n; ++j) {
+            cinv[cord[j]] = j;
+            c_ext[col_off[k] + j] = cord[j];
+        }
+        for (int i = 0; i < m; ++i) {
+            const int old = rord[i];
+            r_ext[row_off[k] + i] = old;
+            for (int e = rp[old]; e < rp[old + 1]; ++e) {
+                gci[pos] = (int32_t)(cinv[colidx[e0 + e]] + col_off[k]);
+                gval[pos] = vals[e0 + e];
+                ++pos;
+            }
+            grp[row_off[k] + i + 1] = (int32_t)pos;
+        }
+        // slice pointers: matrix k owns nslices + 1 entries
+        rs_off[k] = (int64_t)r_sptr.size();
+        for (int s0 = 0; s0 < m; s0 += 32) {
+            r_sptr.push_back(r_pad);
+            r_pad += 32LL * rlen[rord[s0]];
+        }
+        r_sptr.push_back(r_pad);
+        cs_off[k] = (int64_t)c_sptr.size();
+        for (int s0 = 0; s0 < n; s0 += 32) {
+            c_sptr.push_back(c_pad);
+            c_pad += 32LL * clen[cord[s0]];
+        }
+        c_sptr.push_back(c_pad);
         rp_base += m + 1;
     }
     w->h_mat_m.assign(mat_m, mat_m + nmat);
@@ -1106,20 +1315,32 @@ int b2p_batch_upload(void* p, int nmat, const int32_t* mat_m, const int32_t* mat
     std::stable_sort(w->order.begin(), w->order.end(),
                      [&](int a, int b2) { return inst_nnz[a] > inst_nnz[b2]; });
     cudaStream_t s = ctx->stream;
-    for (auto* bf : {&w->rowptr}) B2P_CUDA(ctx, bf->reserve(tm + 1));
+    B2P_CUDA(ctx, w->rowptr.reserve(tm + 1));
     B2P_CUDA(ctx, w->t_rowptr.reserve(tn + 1));
     for (auto* bf : {&w->colidx, &w->t_colidx}) B2P_CUDA(ctx, bf->reserve(nnz));
     for (auto* bf : {&w->vals, &w->t_vals, &w->sv64, &w->stv64}) B2P_CUDA(ctx, bf->reserve(nnz));
     for (auto* bf : {&w->sv32, &w->stv32}) B2P_CUDA(ctx, bf->reserve(nnz));
     for (auto* bf : {&w->dr, &w->pu}) B2P_CUDA(ctx, bf->reserve(tm));
     for (auto* bf : {&w->dc, &w->pv}) B2P_CUDA(ctx, bf->reserve(tn));
+    B2P_CUDA(ctx, w->r_ext.reserve(tm));
+    B2P_CUDA(ctx, w->c_ext.reserve(tn));
     for (auto* bf : {&w->mat_m, &w->mat_n}) B2P_CUDA(ctx, bf->reserve(nmat));
-    for (auto* bf : {&w->mat_row_off, &w->mat_col_off}) B2P_CUDA(ctx, bf->reserve(nmat));
+    for (auto* bf : {&w->mat_row_off, &w->mat_col_off, &w->mat_rs_off, &w->mat_cs_off}) B2P_CUDA(ctx, bf->reserve(nmat));
+    B2P_CUDA(ctx, w->r_sptr.reserve(r_sptr.size()));
+    B2P_CUDA(ctx, w->c_sptr.reserve(c_sptr.size()));
+    B2P_CUDA(ctx, w->r_eidx.reserve(r_pad));
+    B2P_CUDA(ctx, w->c_eidx.reserve(c_pad));
+    B2P_CUDA(ctx, w->r_ev64.reserve(r_pad));
+    B2P_CUDA(ctx, w->c_ev64.reserve(c_pad));
+    B2P_CUDA(ctx, w->r_ev32.reserve(r_pad));
+    B2P_CUDA(ctx, w->c_ev32.reserve(c_pad));
     B2P_CUDA(ctx, w->mat_eta.reserve(nmat));
     B2P_CUDA(ctx, w->inst_mat.reserve(count));
     for (auto* bf : {&w->x_off, &w->y_off}) B2P_CUDA(ctx, bf->reserve(count));
-    for (auto* bf : {&w->c, &w->lb, &w->ub, &w->cs, &w->ls, &w->us, &w->x, &w->xa, &w->xt}) B2P_CUDA(ctx, bf->reserve(IN));
-    for (auto* bf : {&w->b, &w->bs, &w->y, &w->ya, &w->yt}) B2P_CUDA(ctx, bf->reserve(IM));
+    for (auto* bf : {&w->c, &w->lb, &w->ub, &w->x, &w->xt}) B2P_CUDA(ctx, bf->reserve(IN));
+    for (auto* bf : {&w->b, &w->y, &w->yt}) B2P_CUDA(ctx, bf->reserve(IM));
+    B2P_CUDA(ctx, w->colp.reserve(4 * IN));
+    B2P_CUDA(ctx, w->rowp.reserve(4 * IM));
     B2P_CUDA(ctx, w->is_eq.reserve(IM));
     for (auto* bf : {&w->bnorm, &w->cnorm}) B2P_CUDA(ctx, bf->reserve(count));
     B2P_CUDA(ctx, w->ictrl.reserve(count));
@@ -1127,7 +1348,13 @@ int b2p_batch_upload(void* p, int nmat, const int32_t* mat_m, const int32_t* mat
     B2P_CUDA(ctx, w->counters.reserve(2));
     B2P_CUDA(ctx, cudaMemcpyAsync(w->rowptr.p, grp.data(), sizeof(int32_t) * (tm + 1), cudaMemcpyHostToDevice, s));
     B2P_CUDA(ctx, cudaMemcpyAsync(w->colidx.p, gci.data(), sizeof(int32_t) * nnz, cudaMemcpyHostToDevice, s));
-    B2P_CUDA(ctx, cudaMemcpyAsync(w->vals.p, vals, sizeof(double) * nnz, cudaMemcpyHostToDevice, s));
+    B2P_CUDA(ctx, cudaMemcpyAsync(w->vals.p, gval.data(), sizeof(double) * nnz, cudaMemcpyHostToDevice, s));
+    B2P_CUDA(ctx, cudaMemcpyAsync(w->r_ext.p, r_ext.data(), sizeof(int32_t) * tm, cudaMemcpyHostToDevice, s));
+    B2P_CUDA(ctx, cudaMemcpyAsync(w->c_ext.p, c_ext.data(), sizeof(int32_t) * tn, cudaMemcpyHostToDevice, s));
+    B2P_CUDA(ctx, cudaMemcpyAsync(w->r_sptr.p, r_sptr.data(), sizeof(int64_t) * r_sptr.size(), cudaMemcpyHostToDevice, s));
+    B2P_CUDA(ctx, cudaMemcpyAsync(w->c_sptr.p, c_sptr.data(), sizeof(int64_t) * c_sptr.size(), cudaMemcpyHostToDevice, s));
+    B2P_CUDA(ctx, cudaMemcpyAsync(w->mat_rs_off.p, rs_off.data(), sizeof(int64_t) * nmat, cudaMemcpyHostToDevice, s));
+    B2P_CUDA(ctx, cudaMemcpyAsync(w->mat_cs_off.p, cs_off.data(), sizeof(int64_t) * nmat, cudaMemcpyHostToDevice, s));
     B2P_CUDA(ctx, cudaMemcpyAsync(w->mat_m.p, mat_m, sizeof(int32_t) * nmat, cudaMemcpyHostToDevice, s));
     B2P_CUDA(ctx, cudaMemcpyAsync(w->mat_n.p, mat_n, sizeof(int32_t) * nmat, cudaMemcpyHostToDevice, s));
     B2P_CUDA(ctx, cudaMemcpyAsync(w->mat_row_off.p, row_off.data(), sizeof(int64_t) * nmat, cudaMemcpyHostToDevice, s));
@@ -1135,15 +1362,29 @@ int b2p_batch_upload(void* p, int nmat, const int32_t* mat_m, const int32_t* mat
     B2P_CUDA(ctx, cudaMemcpyAsync(w->inst_mat.p, inst_mat, sizeof(int32_t) * count, cudaMemcpyHostToDevice, s));
     B2P_CUDA(ctx, cudaMemcpyAsync(w->x_off.p, xoff.data(), sizeof(int64_t) * count, cudaMemcpyHostToDevice, s));
     B2P_CUDA(ctx, cudaMemcpyAsync(w->y_off.p, yoff.data(), sizeof(int64_t) * count, cudaMemcpyHostToDevice, s));
-    B2P_CUDA(ctx, cudaMemcpyAsync(w->c.p, c, sizeof(double) * IN, cudaMemcpyHostToDevice, s));
-    B2P_CUDA(ctx, cudaMemcpyAsync(w->lb.p, lb, sizeof(double) * IN, cudaMemcpyHostToDevice, s));
-    B2P_CUDA(ctx, cudaMemcpyAsync(w->ub.p, ub, sizeof(double) * IN, cudaMemcpyHostToDevice, s));
-    B2P_CUDA(ctx, cudaMemcpyAsync(w->b.p, b, sizeof(double) * IM, cudaMemcpyHostToDevice, s));
-    B2P_CUDA(ctx, cudaMemcpyAsync(w->is_eq.p, is_eq, IM, cudaMemcpyHostToDevice, s));
+    {
+        // per-instance vectors arrive in external order: stage, then permute on the device
+        DBuf<double> sb, scv, sl, su;
+        DBuf<uint8_t> seq;
+        for (auto* bf : {&scv, &sl, &su}) B2P_CUDA(ctx, bf->reserve(IN));
+        B2P_CUDA(ctx, sb.reserve(IM));
+        B2P_CUDA(ctx, seq.reserve(IM));
+        B2P_CUDA(ctx, cudaMemcpyAsync(scv.p, c, sizeof(double) * IN, cudaMemcpyHostToDevice, s));
+        B2P_CUDA(ctx, cudaMemcpyAsync(sl.p, lb, sizeof(double) * IN, cudaMemcpyHostToDevice, s));
+        B2P_CUDA(ctx, cudaMemcpyAsync(su.p, ub, sizeof(double) * IN, cudaMemcpyHostToDevice, s));
+        B2P_CUDA(ctx, cudaMemcpyAsync(sb.p, b, sizeof(double) * IM, cudaMemcpyHostToDevice, s));
+        B2P_CUDA(ctx, cudaMemcpyAsync(seq.p, is_eq, IM, cudaMemcpyHostToDevice, s));
+        k_permute_inst<<<std::min(count, ctx->sm_count * 8), 256, 0, s>>>(
+            count, w->inst_mat.p, w->mat_m.p, w->mat_n.p, w->mat_row_off.p, w->mat_col_off.p, w->x_off.p, w->y_off.p,
+            w->r_ext.p, w->c_ext.p, sb.p, scv.p, sl.p, su.p, seq.p, w->b.p, w->c.p, w->lb.p, w->ub.p, w->is_eq.p);
+        B2P_LAUNCH(ctx);
+        ctx->launches += 1;
+        B2P_CUDA(ctx, cudaStreamSynchronize(s));  // staging buffers are released at scope end
+    }
     int st = build_transpose(ctx, (int)tm, (int)tn, nnz, w->rowptr.p, w->colidx.p, w->vals.p, w->t_rowptr.p,
                              w->t_colidx.p, w->t_vals.p);
     if (st) return st;
-    // scaling + scaled values + step sizes (per matrix, FP64)
+    // scaling + scaled values + step sizes (per matrix, FP64), then the SELL-32 copies
     DBuf<double> tr, tc;
     B2P_CUDA(ctx, tr.reserve(tm));
     B2P_CUDA(ctx, tc.reserve(tn));
@@ -1158,8 +1399,14 @@ int b2p_batch_upload(void* p, int nmat, const int32_t* mat_m, const int32_t* mat
     k_batch_power<<<gmat, 256, 0, s>>>(nmat, w->mat_m.p, w->mat_n.p, w->mat_row_off.p, w->mat_col_off.p, w->rowptr.p,
                                         w->colidx.p, w->sv64.p, w->t_rowptr.p, w->t_colidx.p, w->stv64.p, w->pv.p,
                                         w->pu.p, 0.998, w->mat_eta.p);
+    k_fill_ell<<<gmat, 256, 0, s>>>(nmat, w->mat_m.p, w->mat_row_off.p, w->mat_col_off.p, w->mat_rs_off.p, w->r_sptr.p,
+                                     w->rowptr.p, w->colidx.p, w->sv64.p, w->sv32.p, w->r_eidx.p, w->r_ev64.p,
+                                     w->r_ev32.p);
+    k_fill_ell<<<gmat, 256, 0, s>>>(nmat, w->mat_n.p, w->mat_col_off.p, w->mat_row_off.p, w->mat_cs_off.p, w->c_sptr.p,
+                                     w->t_rowptr.p, w->t_colidx.p, w->stv64.p, w->stv32.p, w->c_eidx.p, w->c_ev64.p,
+                                     w->c_ev32.p);
     B2P_LAUNCH(ctx);
-    ctx->launches += 3;
+    ctx->launches += 5;
     B2P_CUDA(ctx, cudaStreamSynchronize(s));
     return B2P_OK;
 }
