@@ -242,6 +242,37 @@ int b2p_mlp_set_params(void* ctx, const float* flat);
 /* Mean-squared-error loss of one batch and its gradient (flat layout as above),
  * computed by the same tensor-core forward / backward the training step uses. */
 int b2p_mlp_gradient(void* ctx, const float* X, const float* Y, int N, float* loss_out, float* grad_flat);
+/* Training set on the device from the answers of the last b2p_batch_solve: the
+ * inputs are the instances' parameter vectors (count x in_dim, FP32 host, one per
+ * instance of the batch), the targets their [x (n), y (m), log(final primal
+ * weight)] in the original space, so out_dim must be n + m + 1 and every
+ * instance of the batch must share that shape.  Sets the normalisation
+ * (per-column means; one scale per block x / y / weight).  No solution data
+ * crosses to the host.  No reference counterpart (the reference has no learned
+ * component). */
+int b2p_mlp_dataset_from_batch(void* ctx, const float* features, int count);
+/* `epochs` passes of Adam over the device training set, reshuffled every epoch
+ * (seeded), learning rate cosine-annealed from lr_start to lr_end.  loss_out
+ * (optional): mean squared error of the last epoch, in normalised units. */
+int b2p_mlp_train(void* ctx, int epochs, int batch, float lr_start, float lr_end, uint64_t seed, float* loss_out);
+/* Normalisation used by the dataset and the learned solve: in_mean/in_std
+ * [in_dim], out_mean/out_std [out_dim] (with the weights, a trained model). */
+int b2p_mlp_get_normalization(void* ctx, float* in_mean, float* in_std, float* out_mean, float* out_std);
+int b2p_mlp_set_normalization(void* ctx, const float* in_mean, const float* in_std, const float* out_mean,
+                              const float* out_std);
+/* Learned warm start, all on the device: the MLP maps every instance's parameter
+ * vector (features: count x in_dim, FP32 host) to x0, y0 and a primal weight, the
+ * batch is solved from there (params->precision; default FP32 + re-centring), and
+ * with `fallback` != 0 every instance the warm-started run did not solve is
+ * solved again from the cold start.  Outputs as b2p_batch_solve, plus
+ * warm_used_out[i] = 1 when instance i's answer came from the warm start; the
+ * iteration count of a fallen-back instance includes its warm-started run.
+ * summary->refinement_rounds_done = number of instances that fell back.  Replaces
+ * the reference's cold-start-only GPUFirstOrderSolver::solve
+ * (src/first_order_solver.cpp:295-306) for parametric families. */
+int b2p_batch_solve_learned(void* ctx, const b2p_params* params, const float* features, int fallback,
+                            int32_t* status_out, int64_t* iters_out, double* kkt_out, uint8_t* warm_used_out,
+                            double* x_out, double* y_out, b2p_result* summary);
 /* Raw BF16 GEMM on the tensor cores, for tests: C(MxN, fp32) = op(A) op(B),
  * A is M x K (trans_a = 0) or K x M (trans_a = 1) bf16 row-major, B is K x N
  * (trans_b = 0) or N x K (trans_b = 1).  Host buffers (bf16 as uint16). */

@@ -14,6 +14,7 @@ from pathlib import Path
 import numpy as np
 
 from . import lpgen  # noqa: F401  (workload generators)
+from . import warmstart  # noqa: F401  (learned warm start orchestration)
 
 _HERE = Path(__file__).resolve().parent
 LIB_PATH = Path(os.environ.get("B2P_LIB", _HERE / "libb2p.so"))
@@ -99,6 +100,12 @@ SIGNATURES = {
     "b2p_mlp_set_params": (C.c_int, [_P, _F32P]),
     "b2p_mlp_gradient": (C.c_int, [_P, _F32P, _F32P, C.c_int, C.POINTER(C.c_float), _F32P]),
     "b2p_gemm_bf16": (C.c_int, [_P, C.c_int, C.c_int, C.c_int, _U16P, C.c_int, _U16P, C.c_int, _F32P]),
+    "b2p_mlp_dataset_from_batch": (C.c_int, [_P, _F32P, C.c_int]),
+    "b2p_mlp_train": (C.c_int, [_P, C.c_int, C.c_int, C.c_float, C.c_float, C.c_uint64, C.POINTER(C.c_float)]),
+    "b2p_mlp_get_normalization": (C.c_int, [_P, _F32P, _F32P, _F32P, _F32P]),
+    "b2p_mlp_set_normalization": (C.c_int, [_P, _F32P, _F32P, _F32P, _F32P]),
+    "b2p_batch_solve_learned": (C.c_int, [_P, C.POINTER(Params), _F32P, C.c_int, _P, _P, _P, _P, _P, _P,
+                                          C.POINTER(Result)]),
 }
 
 _lib = None
@@ -275,15 +282,17 @@ class Context:
                                            np.ascontiguousarray(ub, np.float64),
                                            np.ascontiguousarray(is_eq, np.uint8)))
 
-    def batch_solve(self, x0=None, y0=None, omega0=None, **params):
+    def batch_solve(self, x0=None, y0=None, omega0=None, outputs=True, **params):
+        """Solve every uploaded instance (b2p_batch_solve).  outputs=False skips the
+        host copies of x and y (the answers stay on the device, e.g. as training labels)."""
         p = default_params(engine="halpern", **params)
         cnt = len(self.batch_m)
         st = np.zeros(cnt, np.int32)
         it = np.zeros(cnt, np.int64)
         kk = np.zeros(cnt)
         omo = np.zeros(cnt)
-        x = np.zeros(int(self.batch_n.sum()))
-        y = np.zeros(int(self.batch_m.sum()))
+        x = np.zeros(int(self.batch_n.sum())) if outputs else None
+        y = np.zeros(int(self.batch_m.sum())) if outputs else None
         r = Result()
         x0 = None if x0 is None else np.ascontiguousarray(x0, np.float64)
         y0 = None if y0 is None else np.ascontiguousarray(y0, np.float64)
@@ -291,6 +300,26 @@ class Context:
         self._check(lib().b2p_batch_solve(self._h, C.byref(p), _ptr(x0), _ptr(y0), _ptr(om), _ptr(st), _ptr(it),
                                           _ptr(kk), _ptr(omo), _ptr(x), _ptr(y), C.byref(r)))
         return _result_dict(r), {"status": st, "iterations": it, "rel_kkt": kk, "omega": omo}, x, y
+
+    def batch_solve_learned(self, features, fallback=True, outputs=True, **params):
+        """Learned warm start for every instance of the uploaded batch (see
+        b2p_batch_solve_learned): MLP inference, warm-started solve, cold fallback."""
+        params.setdefault("precision", "fp32")
+        p = default_params(engine="halpern", **params)
+        cnt = len(self.batch_m)
+        F = np.ascontiguousarray(features, np.float32)
+        st = np.zeros(cnt, np.int32)
+        it = np.zeros(cnt, np.int64)
+        kk = np.zeros(cnt)
+        used = np.zeros(cnt, np.uint8)
+        x = np.zeros(int(self.batch_n.sum())) if outputs else None
+        y = np.zeros(int(self.batch_m.sum())) if outputs else None
+        r = Result()
+        self._check(lib().b2p_batch_solve_learned(self._h, C.byref(p), F, 1 if fallback else 0, _ptr(st), _ptr(it),
+                                                  _ptr(kk), _ptr(used), _ptr(x), _ptr(y), C.byref(r)))
+        summ = _result_dict(r)
+        summ["fallbacks"] = r.refinement_rounds_done
+        return summ, {"status": st, "iterations": it, "rel_kkt": kk, "warm_used": used}, x, y
 
     # ---- MLP
     def mlp_create(self, in_dim, hidden, out_dim, seed=0):
@@ -304,6 +333,26 @@ class Context:
         Y = np.ascontiguousarray(Y, np.float32)
         self._check(lib().b2p_mlp_train_epoch(self._h, X, Y, X.shape[0], batch, lr, C.byref(loss)))
         return loss.value
+
+    def mlp_dataset_from_batch(self, features):
+        F = np.ascontiguousarray(features, np.float32)
+        self._check(lib().b2p_mlp_dataset_from_batch(self._h, F, F.shape[0]))
+
+    def mlp_train(self, epochs, batch=256, lr_start=1e-3, lr_end=1e-5, seed=0):
+        loss = C.c_float()
+        self._check(lib().b2p_mlp_train(self._h, epochs, batch, lr_start, lr_end, seed, C.byref(loss)))
+        return loss.value
+
+    def mlp_get_normalization(self):
+        i, _, o = self.mlp_dims
+        a, b, c, d = (np.zeros(i, np.float32), np.zeros(i, np.float32), np.zeros(o, np.float32),
+                      np.zeros(o, np.float32))
+        self._check(lib().b2p_mlp_get_normalization(self._h, a, b, c, d))
+        return a, b, c, d
+
+    def mlp_set_normalization(self, in_mean, in_std, out_mean, out_std):
+        arr = [np.ascontiguousarray(v, np.float32) for v in (in_mean, in_std, out_mean, out_std)]
+        self._check(lib().b2p_mlp_set_normalization(self._h, *arr))
 
     def mlp_infer(self, X):
         X = np.ascontiguousarray(X, np.float32)

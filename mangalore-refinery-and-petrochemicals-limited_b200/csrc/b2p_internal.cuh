@@ -133,6 +133,12 @@ void halpern_free(Ctx* ctx);
 void batch_free(Ctx* ctx);
 void mlp_free(Ctx* ctx);
 
+// Learned warm start (mlp.cu), used by the batch engine: training set from a batched
+// solve's answers (device, external order), and warm starts predicted on the device.
+int mlp_set_dataset(Ctx* ctx, const float* feat_host, int count, int n, int m, const double* x_dev,
+                    const double* y_dev, const double* om_dev);
+int mlp_predict_warm(Ctx* ctx, const float* feat_host, int count, int n, int m, double* x0, double* y0, double* om);
+
 // ---------------------------------------------------------------- device helpers
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll

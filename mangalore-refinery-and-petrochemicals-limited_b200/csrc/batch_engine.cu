@@ -103,6 +103,13 @@ struct BatchWork {
     DBuf<int32_t> active, active2, counters;  // counters[0]=head, [1]=active count
     std::vector<int32_t> h_inst_mat, order;
     int max_m = 0, max_n = 0;
+    // results of the last solve: per-instance control blocks (host) and the answers
+    // in the original space, external order (device, FP64), with the primal weights
+    std::vector<InstCtrl> hc;
+    DBuf<double> ox, oy, oom;
+    bool solved = false;
+    int tuned_threads[2] = {0, 0};  // block size per precision (0 = not tuned yet)
+    DBuf<int32_t> list;             // instances re-initialised by a subset solve
 };
 
 void batch_free(Ctx* ctx) {
@@ -742,17 +749,19 @@ __global__ void k_permute_inst(int count, const int32_t* __restrict__ inst_mat, 
 }
 
 // Per-instance norms, initial point, packed records and control block (CTA per
-// instance).  Warm starts arrive in external order.  With re-centring the initial
+// instance; all `count` instances, or those named by `list`).  Warm starts arrive
+// in external order.  With re-centring the initial
 // point (warm start, else the bound projection of 0) becomes the first FP64
 // centre and the iterates start at 0.
 template <typename MT>
-__global__ void k_batch_init(BArgs a, int count, const double* __restrict__ x0, const double* __restrict__ y0,
-                             const double* __restrict__ omega0) {
+__global__ void k_batch_init(BArgs a, int count, const int32_t* __restrict__ list, const double* __restrict__ x0,
+                             const double* __restrict__ y0, const double* __restrict__ omega0) {
     __shared__ double red[32 * 4];
     ColP<MT>* colp = (ColP<MT>*)a.colp;
     RowP<MT>* rowp = (RowP<MT>*)a.rowp;
     MT *xg = (MT*)a.x, *xtg = (MT*)a.xt, *yg = (MT*)a.y, *ytg = (MT*)a.yt;
-    for (int inst = blockIdx.x; inst < count; inst += gridDim.x) {
+    for (int q = blockIdx.x; q < count; q += gridDim.x) {
+        const int inst = list ? list[q] : q;
         const int k = a.inst_mat[inst];
         const int m = a.mat_m[k], n = a.mat_n[k];
         const int64_t ro = a.mat_row_off[k], co = a.mat_col_off[k], xo = a.x_off[inst], yo = a.y_off[inst];
@@ -962,10 +971,11 @@ size_t smem_bytes(BatchWork* w, size_t mt_size) {
 
 template <typename MT>
 int init_instances(Ctx* ctx, BatchWork* w, const b2p_params* p, const double* x0_dev, const double* y0_dev,
-                   const double* om_dev) {
-    int grid = std::min(w->count, ctx->sm_count * 8);
+                   const double* om_dev, const int32_t* list_dev = nullptr, int list_count = 0) {
+    const int cnt = list_dev ? list_count : w->count;
+    int grid = std::min(cnt, ctx->sm_count * 8);
     BArgs a = make_args<MT>(w, p, w->active.p);
-    k_batch_init<MT><<<grid, 256, 0, ctx->stream>>>(a, w->count, x0_dev, y0_dev, om_dev);
+    k_batch_init<MT><<<grid, 256, 0, ctx->stream>>>(a, cnt, list_dev, x0_dev, y0_dev, om_dev);
     B2P_LAUNCH(ctx);
     ctx->launches += 1;
     return B2P_OK;
@@ -1022,31 +1032,25 @@ int autotune(Ctx* ctx, BatchWork* w, const b2p_params* p, TuneCfg* best) {
 }
 
 template <typename MT>
-int batch_run(Ctx* ctx, BatchWork* w, const b2p_params* p, const double* x0, const double* y0, const double* omega0,
-              int32_t* status_out, int64_t* iters_out, double* kkt_out, double* omega_out, double* x_out, double* y_out,
-              b2p_result* sum) {
+int batch_run(Ctx* ctx, BatchWork* w, const b2p_params* p, const double* x0_dev, const double* y0_dev,
+              const double* om_dev, const std::vector<int32_t>* subset, bool* timed_out_out, float* kms_out,
+              TuneCfg* cfg_out) {
     cudaStream_t s = ctx->stream;
     double t_start = now_ms();
     const int64_t IN = w->inst_n, IM = w->inst_m;
+    const int prec = sizeof(MT) == 8 ? 0 : 1;
     w->recenter = false;  // autotune trials run without re-centring
     TuneCfg cfg = {256, 2048};
-    {
+    if (w->tuned_threads[prec] > 0) {
+        cfg.threads = w->tuned_threads[prec];
+    } else {
+        if (subset) {
+            ctx->err = "subset solve before a full solve of this precision";
+            return B2P_INVALID_ARGUMENT;
+        }
         int st = autotune<MT>(ctx, w, p, &cfg);
         if (st) return st;
-    }
-    // warm starts / weights
-    DBuf<double> dx0, dy0, dom;
-    if (x0) {
-        B2P_CUDA(ctx, dx0.reserve(IN));
-        B2P_CUDA(ctx, cudaMemcpyAsync(dx0.p, x0, sizeof(double) * IN, cudaMemcpyHostToDevice, s));
-    }
-    if (y0) {
-        B2P_CUDA(ctx, dy0.reserve(IM));
-        B2P_CUDA(ctx, cudaMemcpyAsync(dy0.p, y0, sizeof(double) * IM, cudaMemcpyHostToDevice, s));
-    }
-    if (omega0) {
-        B2P_CUDA(ctx, dom.reserve(w->count));
-        B2P_CUDA(ctx, cudaMemcpyAsync(dom.p, omega0, sizeof(double) * w->count, cudaMemcpyHostToDevice, s));
+        w->tuned_threads[prec] = cfg.threads;
     }
     // re-centring: on by default for the mixed engine (refinement_rounds < 0), forced by > 0
     w->recenter = p->refinement_rounds > 0 || (p->refinement_rounds < 0 && sizeof(MT) == 4);
@@ -1054,11 +1058,31 @@ int batch_run(Ctx* ctx, BatchWork* w, const b2p_params* p, const double* x0, con
         for (auto* b : {&w->xbar, &w->atybar}) B2P_CUDA(ctx, b->reserve(IN));
         for (auto* b : {&w->ybar, &w->axbar}) B2P_CUDA(ctx, b->reserve(IM));
     }
-    int st = init_instances<MT>(ctx, w, p, x0 ? dx0.p : nullptr, y0 ? dy0.p : nullptr, omega0 ? dom.p : nullptr);
-    if (st) return st;
-    // active list = all instances, longest first
-    B2P_CUDA(ctx, cudaMemcpyAsync(w->active.p, w->order.data(), sizeof(int32_t) * w->count, cudaMemcpyHostToDevice, s));
-    int32_t cnt[2] = {0, w->count};
+    // instances to run, longest first
+    std::vector<int32_t> act;
+    if (subset) {
+        std::vector<uint8_t> in_set(w->count, 0);
+        for (int32_t i : *subset) in_set[i] = 1;
+        for (int32_t i : w->order)
+            if (in_set[i]) act.push_back(i);
+        if (act.empty()) {
+            if (timed_out_out) *timed_out_out = false;
+            if (kms_out) *kms_out = 0.0f;
+            if (cfg_out) *cfg_out = cfg;
+            return B2P_OK;
+        }
+        B2P_CUDA(ctx, w->list.reserve(act.size()));
+        B2P_CUDA(ctx, cudaMemcpyAsync(w->list.p, act.data(), sizeof(int32_t) * act.size(), cudaMemcpyHostToDevice, s));
+        int st = init_instances<MT>(ctx, w, p, x0_dev, y0_dev, om_dev, w->list.p, (int)act.size());
+        if (st) return st;
+    } else {
+        act = w->order;
+        int st = init_instances<MT>(ctx, w, p, x0_dev, y0_dev, om_dev);
+        if (st) return st;
+    }
+    const int n_act = (int)act.size();
+    B2P_CUDA(ctx, cudaMemcpyAsync(w->active.p, act.data(), sizeof(int32_t) * n_act, cudaMemcpyHostToDevice, s));
+    int32_t cnt[2] = {0, n_act};
     B2P_CUDA(ctx, cudaMemcpyAsync(w->counters.p, cnt, sizeof(cnt), cudaMemcpyHostToDevice, s));
     size_t sm = smem_bytes(w, sizeof(MT));
     auto fn = k_batch_chunk<MT>;
@@ -1117,46 +1141,76 @@ int batch_run(Ctx* ctx, BatchWork* w, const b2p_params* p, const double* x0, con
     ctx->launches += graphs * 4;
     float kms = 0;
     cudaEventElapsedTime(&kms, ctx->ev0, ctx->ev1);
-    // results
-    std::vector<InstCtrl> hc(w->count);
-    B2P_CUDA(ctx, cudaMemcpyAsync(hc.data(), w->ictrl.p, sizeof(InstCtrl) * w->count, cudaMemcpyDeviceToHost, s));
-    if (x_out || y_out) {
-        DBuf<double> ox, oy;
-        B2P_CUDA(ctx, ox.reserve(IN));
-        B2P_CUDA(ctx, oy.reserve(IM));
-        k_batch_unscale<MT><<<std::min(w->count, ctx->sm_count * 8), 256, 0, s>>>(
-            a1, w->count, w->recenter ? w->xbar.p : nullptr, w->recenter ? w->ybar.p : nullptr, ox.p, oy.p);
-        B2P_LAUNCH(ctx);
-        ctx->launches += 1;
-        if (x_out) B2P_CUDA(ctx, cudaMemcpyAsync(x_out, ox.p, sizeof(double) * IN, cudaMemcpyDeviceToHost, s));
-        if (y_out) B2P_CUDA(ctx, cudaMemcpyAsync(y_out, oy.p, sizeof(double) * IM, cudaMemcpyDeviceToHost, s));
-    }
+    // results of every instance: control blocks to the host, answers (original space,
+    // external order) and primal weights kept on the device
+    w->hc.resize(w->count);
+    B2P_CUDA(ctx, cudaMemcpyAsync(w->hc.data(), w->ictrl.p, sizeof(InstCtrl) * w->count, cudaMemcpyDeviceToHost, s));
+    B2P_CUDA(ctx, w->ox.reserve(IN));
+    B2P_CUDA(ctx, w->oy.reserve(IM));
+    B2P_CUDA(ctx, w->oom.reserve(w->count));
+    k_batch_unscale<MT><<<std::min(w->count, ctx->sm_count * 8), 256, 0, s>>>(
+        a1, w->count, w->recenter ? w->xbar.p : nullptr, w->recenter ? w->ybar.p : nullptr, w->ox.p, w->oy.p);
+    B2P_LAUNCH(ctx);
+    ctx->launches += 1;
     B2P_CUDA(ctx, cudaStreamSynchronize(s));
-    int64_t tot_it = 0, opt = 0, maxit = 0;
-    double worst = 0;
+    std::vector<double> om(w->count);
+    for (int i = 0; i < w->count; ++i) om[i] = w->hc[i].omega;
+    B2P_CUDA(ctx, cudaMemcpyAsync(w->oom.p, om.data(), sizeof(double) * w->count, cudaMemcpyHostToDevice, s));
+    B2P_CUDA(ctx, cudaStreamSynchronize(s));
+    w->solved = true;
+    if (timed_out_out) *timed_out_out = timed_out;
+    if (kms_out) *kms_out = kms;
+    if (cfg_out) *cfg_out = cfg;
+    return B2P_OK;
+}
+
+// Per-instance outputs of the last solve (any pointer may be null).
+int collect_outputs(Ctx* ctx, BatchWork* w, bool timed_out, int32_t* status_out, int64_t* iters_out, double* kkt_out,
+                    double* omega_out, double* x_out, double* y_out, int64_t* tot_it, int64_t* maxit, int64_t* opt,
+                    double* worst) {
+    cudaStream_t s = ctx->stream;
+    *tot_it = 0;
+    *maxit = 0;
+    *opt = 0;
+    *worst = 0.0;
     for (int i = 0; i < w->count; ++i) {
-        const InstCtrl& c = hc[i];
+        const InstCtrl& c = w->hc[i];
         int stt = c.done ? c.status : (timed_out ? B2P_STATUS_INTERRUPTED : B2P_STATUS_MAX_ITERATIONS);
         double kk = std::max(c.rel_p, std::max(c.rel_d, c.rel_g));
         if (status_out) status_out[i] = stt;
         if (iters_out) iters_out[i] = c.total;
         if (kkt_out) kkt_out[i] = kk;
         if (omega_out) omega_out[i] = c.omega;
-        tot_it += c.total;
-        maxit = std::max<int64_t>(maxit, c.total);
-        opt += (stt == B2P_STATUS_OPTIMAL);
-        worst = std::max(worst, kk);
+        *tot_it += c.total;
+        *maxit = std::max<int64_t>(*maxit, c.total);
+        *opt += (stt == B2P_STATUS_OPTIMAL);
+        *worst = std::max(*worst, kk);
     }
-    if (sum) {
-        sum->status = (opt == w->count) ? B2P_STATUS_OPTIMAL : (timed_out ? B2P_STATUS_INTERRUPTED : B2P_STATUS_MAX_ITERATIONS);
-        sum->iterations = tot_it;   // sum over instances
-        sum->restarts = maxit;      // longest instance
-        sum->rel_kkt = worst;
-        sum->kernel_time_ms = kms;
-        sum->primal_weight = 0.0;
-        sum->step_size = cfg.threads * 100000.0 + cfg.chunk;  // tuned block size * 1e5 + chunk length
-    }
+    if (x_out) B2P_CUDA(ctx, cudaMemcpyAsync(x_out, w->ox.p, sizeof(double) * w->inst_n, cudaMemcpyDeviceToHost, s));
+    if (y_out) B2P_CUDA(ctx, cudaMemcpyAsync(y_out, w->oy.p, sizeof(double) * w->inst_m, cudaMemcpyDeviceToHost, s));
+    B2P_CUDA(ctx, cudaStreamSynchronize(s));
     return B2P_OK;
+}
+
+void fill_summary(b2p_result* sum, int count, bool timed_out, int64_t tot_it, int64_t maxit, int64_t opt, double worst,
+                  float kms, const TuneCfg& cfg) {
+    if (!sum) return;
+    sum->status = (opt == count) ? B2P_STATUS_OPTIMAL : (timed_out ? B2P_STATUS_INTERRUPTED : B2P_STATUS_MAX_ITERATIONS);
+    sum->iterations = tot_it;  // sum over instances
+    sum->restarts = maxit;     // longest instance
+    sum->rel_kkt = worst;
+    sum->kernel_time_ms = kms;
+    sum->primal_weight = 0.0;
+    sum->step_size = cfg.threads * 100000.0 + cfg.chunk;  // tuned block size * 1e5 + chunk length
+}
+
+// All instances of the batch share one shape (required by the learned warm start).
+bool uniform_shape(BatchWork* w, int* n, int* m) {
+    *n = w->h_mat_n[w->h_inst_mat[0]];
+    *m = w->h_mat_m[w->h_inst_mat[0]];
+    for (int i = 1; i < w->count; ++i)
+        if (w->h_mat_n[w->h_inst_mat[i]] != *n || w->h_mat_m[w->h_inst_mat[i]] != *m) return false;
+    return true;
 }
 
 }  // namespace
@@ -1416,7 +1470,8 @@ int b2p_batch_solve(void* p, const b2p_params* params, const double* x0, const d
                     double* y_out, b2p_result* summary) {
     Ctx* ctx = static_cast<Ctx*>(p);
     if (!ctx) return B2P_GPU_UNINITIALIZED;
-    if (!ctx->bw) {
+    BatchWork* w = ctx->bw;
+    if (!w) {
         ctx->err = "b2p_batch_solve: no batch uploaded";
         return B2P_NO_LP;
     }
@@ -1432,16 +1487,147 @@ int b2p_batch_solve(void* p, const b2p_params* params, const double* x0, const d
     if (summary) std::memset(summary, 0, sizeof(*summary));
     int64_t l0 = ctx->launches;
     double t0 = now_ms();
+    cudaStream_t s = ctx->stream;
+    // warm starts / weights to the device
+    DBuf<double> dx0, dy0, dom;
+    if (x0) {
+        B2P_CUDA(ctx, dx0.reserve(w->inst_n));
+        B2P_CUDA(ctx, cudaMemcpyAsync(dx0.p, x0, sizeof(double) * w->inst_n, cudaMemcpyHostToDevice, s));
+    }
+    if (y0) {
+        B2P_CUDA(ctx, dy0.reserve(w->inst_m));
+        B2P_CUDA(ctx, cudaMemcpyAsync(dy0.p, y0, sizeof(double) * w->inst_m, cudaMemcpyHostToDevice, s));
+    }
+    if (omega0) {
+        B2P_CUDA(ctx, dom.reserve(w->count));
+        B2P_CUDA(ctx, cudaMemcpyAsync(dom.p, omega0, sizeof(double) * w->count, cudaMemcpyHostToDevice, s));
+    }
+    bool timed_out = false;
+    float kms = 0.0f;
+    TuneCfg cfg = {0, 0};
     int st = pp->precision == B2P_FP64
-                 ? batch_run<double>(ctx, ctx->bw, pp, x0, y0, omega0, status_out, iters_out, kkt_out, omega_out, x_out,
-                                     y_out, summary)
-                 : batch_run<float>(ctx, ctx->bw, pp, x0, y0, omega0, status_out, iters_out, kkt_out, omega_out, x_out,
-                                    y_out, summary);
+                 ? batch_run<double>(ctx, w, pp, x0 ? dx0.p : nullptr, y0 ? dy0.p : nullptr, omega0 ? dom.p : nullptr,
+                                     nullptr, &timed_out, &kms, &cfg)
+                 : batch_run<float>(ctx, w, pp, x0 ? dx0.p : nullptr, y0 ? dy0.p : nullptr, omega0 ? dom.p : nullptr,
+                                    nullptr, &timed_out, &kms, &cfg);
+    if (st) return st;
+    int64_t tot_it, maxit, opt;
+    double worst;
+    st = collect_outputs(ctx, w, timed_out, status_out, iters_out, kkt_out, omega_out, x_out, y_out, &tot_it, &maxit,
+                         &opt, &worst);
+    if (st) return st;
+    fill_summary(summary, w->count, timed_out, tot_it, maxit, opt, worst, kms, cfg);
     if (summary) {
         summary->solve_time_ms = now_ms() - t0;
         summary->kernel_launches = ctx->launches - l0;
     }
-    return st;
+    return B2P_OK;
+}
+
+int b2p_batch_solve_learned(void* p, const b2p_params* params, const float* features, int fallback,
+                            int32_t* status_out, int64_t* iters_out, double* kkt_out, uint8_t* warm_used_out,
+                            double* x_out, double* y_out, b2p_result* summary) {
+    Ctx* ctx = static_cast<Ctx*>(p);
+    if (!ctx) return B2P_GPU_UNINITIALIZED;
+    BatchWork* w = ctx->bw;
+    if (!w) {
+        ctx->err = "b2p_batch_solve_learned: no batch uploaded";
+        return B2P_NO_LP;
+    }
+    if (!features) {
+        ctx->err = "b2p_batch_solve_learned: null parameter vectors";
+        return B2P_INVALID_ARGUMENT;
+    }
+    int n = 0, m = 0;
+    if (!uniform_shape(w, &n, &m)) {
+        ctx->err = "b2p_batch_solve_learned: the instances of the batch differ in shape";
+        return B2P_INVALID_ARGUMENT;
+    }
+    b2p_params def;
+    b2p_params_default(&def);
+    def.engine = B2P_ENGINE_HALPERN;
+    def.precision = B2P_FP32;
+    const b2p_params* pp = params ? params : &def;
+    if (pp->check_every < 2 || pp->max_iterations < 0) {
+        ctx->err = "b2p_batch_solve_learned: check_every must be >= 2";
+        return B2P_INVALID_ARGUMENT;
+    }
+    cudaSetDevice(ctx->device);
+    if (summary) std::memset(summary, 0, sizeof(*summary));
+    int64_t l0 = ctx->launches;
+    double t0 = now_ms();
+    // warm start from the MLP, on the device
+    DBuf<double> dx0, dy0, dom;
+    B2P_CUDA(ctx, dx0.reserve(w->inst_n));
+    B2P_CUDA(ctx, dy0.reserve(w->inst_m));
+    B2P_CUDA(ctx, dom.reserve(w->count));
+    int st = mlp_predict_warm(ctx, features, w->count, n, m, dx0.p, dy0.p, dom.p);
+    if (st) return st;
+    const bool f64 = pp->precision == B2P_FP64;
+    bool timed_out = false;
+    float kms = 0.0f, kms2 = 0.0f;
+    TuneCfg cfg = {0, 0};
+    st = f64 ? batch_run<double>(ctx, w, pp, dx0.p, dy0.p, dom.p, nullptr, &timed_out, &kms, &cfg)
+             : batch_run<float>(ctx, w, pp, dx0.p, dy0.p, dom.p, nullptr, &timed_out, &kms, &cfg);
+    if (st) return st;
+    // cold-start fallback for every instance the warm-started run did not solve
+    std::vector<int64_t> warm_iters(w->count);
+    std::vector<int32_t> failed;
+    for (int i = 0; i < w->count; ++i) {
+        warm_iters[i] = w->hc[i].total;
+        if (!(w->hc[i].done && w->hc[i].status == B2P_STATUS_OPTIMAL)) failed.push_back(i);
+    }
+    if (fallback && !failed.empty() && !timed_out) {
+        st = f64 ? batch_run<double>(ctx, w, pp, nullptr, nullptr, nullptr, &failed, &timed_out, &kms2, &cfg)
+                 : batch_run<float>(ctx, w, pp, nullptr, nullptr, nullptr, &failed, &timed_out, &kms2, &cfg);
+        if (st) return st;
+    }
+    int64_t tot_it, maxit, opt;
+    double worst;
+    st = collect_outputs(ctx, w, timed_out, status_out, nullptr, kkt_out, nullptr, x_out, y_out, &tot_it, &maxit, &opt,
+                         &worst);
+    if (st) return st;
+    std::vector<uint8_t> is_failed(w->count, 0);
+    if (fallback)
+        for (int32_t i : failed) is_failed[i] = 1;
+    tot_it = 0;
+    maxit = 0;
+    for (int i = 0; i < w->count; ++i) {
+        // iterations spent on the instance: the warm run, plus the cold run when it fell back
+        const int64_t it = is_failed[i] ? warm_iters[i] + w->hc[i].total : w->hc[i].total;
+        if (iters_out) iters_out[i] = it;
+        if (warm_used_out) warm_used_out[i] = is_failed[i] ? 0 : 1;
+        tot_it += it;
+        maxit = std::max(maxit, it);
+    }
+    fill_summary(summary, w->count, timed_out, tot_it, maxit, opt, worst, kms + kms2, cfg);
+    if (summary) {
+        summary->solve_time_ms = now_ms() - t0;
+        summary->kernel_launches = ctx->launches - l0;
+        summary->refinement_rounds_done = fallback ? (int)failed.size() : 0;  // instances that fell back
+    }
+    return B2P_OK;
+}
+
+int b2p_mlp_dataset_from_batch(void* p, const float* features, int count) {
+    Ctx* ctx = static_cast<Ctx*>(p);
+    if (!ctx) return B2P_GPU_UNINITIALIZED;
+    BatchWork* w = ctx->bw;
+    if (!w || !w->solved) {
+        ctx->err = "b2p_mlp_dataset_from_batch: no solved batch";
+        return B2P_NO_LP;
+    }
+    if (!features || count != w->count) {
+        ctx->err = "b2p_mlp_dataset_from_batch: one parameter vector per instance of the batch is required";
+        return B2P_INVALID_ARGUMENT;
+    }
+    int n = 0, m = 0;
+    if (!uniform_shape(w, &n, &m)) {
+        ctx->err = "b2p_mlp_dataset_from_batch: the instances of the batch differ in shape";
+        return B2P_INVALID_ARGUMENT;
+    }
+    cudaSetDevice(ctx->device);
+    return mlp_set_dataset(ctx, features, count, n, m, w->ox.p, w->oy.p, w->oom.p);
 }
 
 }  // extern "C"

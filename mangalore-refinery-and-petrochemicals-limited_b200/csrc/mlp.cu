@@ -27,6 +27,10 @@
 #include <cstring>
 #include <vector>
 
+#include <algorithm>
+#include <numeric>
+#include <random>
+
 #include "b2p_internal.cuh"
 
 namespace b2p {
@@ -45,6 +49,13 @@ struct MlpState {
     DBuf<__nv_bfloat16> Xh, Xt, H1, H1t, H2, H2t, dY, dYt, dZ, dZt;
     DBuf<double> loss;
     DBuf<int> err;
+    // normalisation of inputs and targets: v_norm = (v - mean) / std
+    DBuf<float> in_mean, in_std, out_mean, out_std;
+    bool has_norm = false;
+    // training set resident on the device (normalised, row-major) and the epoch order
+    DBuf<float> DX, DT;
+    DBuf<int32_t> perm;
+    int dcount = 0;
 };
 
 void mlp_free(Ctx* ctx) {
@@ -417,6 +428,83 @@ __global__ void k_init_uniform(long long n, float a, unsigned long long seed, fl
     }
 }
 
+// ---------------------------------------------------------------- learned warm start: data kernels
+// Column mean and std of a row-major [rows x cols] block (two passes, FP64), std
+// floored at floor_rel * (1 + |mean|).  `logit` takes log(max(v, 1e-30)) of every
+// value first (primal weights).
+template <typename T>
+__global__ void k_col_stats(int rows, int cols, const T* __restrict__ src, long long ld, float floor_rel, bool logit,
+                            float* __restrict__ mean, float* __restrict__ stdv) {
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < cols; c += gridDim.x * blockDim.x) {
+        double s = 0.0;
+        for (int r = 0; r < rows; ++r) {
+            double v = (double)src[(size_t)r * ld + c];
+            s += logit ? log(fmax(v, 1e-30)) : v;
+        }
+        const double mu = s / rows;
+        double q = 0.0;
+        for (int r = 0; r < rows; ++r) {
+            double v = (double)src[(size_t)r * ld + c];
+            const double d = (logit ? log(fmax(v, 1e-30)) : v) - mu;
+            q += d * d;
+        }
+        const double sd = sqrt(q / rows);
+        mean[c] = (float)mu;
+        stdv[c] = (float)fmax(sd, floor_rel * (1.0 + fabs(mu)));
+    }
+}
+
+// Normalised training targets [rows x (n + m + 1)]: x (n), y (m), log(primal weight).
+__global__ void k_build_targets(int rows, int n, int m, const double* __restrict__ x, const double* __restrict__ y,
+                                const double* __restrict__ om, const float* __restrict__ mean,
+                                const float* __restrict__ stdv, float* __restrict__ T) {
+    const int out = n + m + 1;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < (long long)rows * out;
+         i += (long long)gridDim.x * blockDim.x) {
+        const int r = (int)(i / out), c = (int)(i % out);
+        const double v = c < n ? x[(size_t)r * n + c]
+                               : (c < n + m ? y[(size_t)r * m + (c - n)] : log(fmax(om[r], 1e-30)));
+        T[i] = (float)((v - (double)mean[c]) / (double)stdv[c]);
+    }
+}
+
+// rows x cols: dst = (src - mean) / std
+__global__ void k_norm_rows(long long count, int cols, const float* __restrict__ src, const float* __restrict__ mean,
+                            const float* __restrict__ stdv, float* __restrict__ dst) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < count * cols;
+         i += (long long)gridDim.x * blockDim.x) {
+        const int c = (int)(i % cols);
+        dst[i] = (src[i] - mean[c]) / stdv[c];
+    }
+}
+
+// dst[r] = src[idx[r]] for r < valid, zero rows up to `rows` (rows x cols, row-major)
+__global__ void k_gather_rows(int valid, int rows, int cols, const int32_t* __restrict__ idx,
+                              const float* __restrict__ src, float* __restrict__ dst) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < (long long)rows * cols;
+         i += (long long)gridDim.x * blockDim.x) {
+        const int r = (int)(i / cols), c = (int)(i % cols);
+        dst[i] = r < valid ? src[(size_t)idx[r] * cols + c] : 0.0f;
+    }
+}
+
+// MLP output rows (ld outp) -> warm start of instances row0 .. row0+valid-1:
+// x0 [n], y0 [m] (external order, FP64) and the primal weight exp(clamped log).
+__global__ void k_denorm_warm(int valid, int outp, int n, int m, const float* __restrict__ Y,
+                              const float* __restrict__ mean, const float* __restrict__ stdv, long long row0,
+                              double* __restrict__ x0, double* __restrict__ y0, double* __restrict__ om) {
+    const int out = n + m + 1;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < (long long)valid * out;
+         i += (long long)gridDim.x * blockDim.x) {
+        const int r = (int)(i / out), c = (int)(i % out);
+        const double v = (double)Y[(size_t)r * outp + c] * (double)stdv[c] + (double)mean[c];
+        const long long g = row0 + r;
+        if (c < n) x0[g * n + c] = v;
+        else if (c < n + m) y0[g * m + (c - n)] = v;
+        else om[g] = exp(fmin(fmax(v, -30.0), 30.0));
+    }
+}
+
 // ---------------------------------------------------------------- MLP host side
 unsigned ew_grid(Ctx* ctx, long long n) { return grid_for(n, 256, ctx->sm_count, 8); }
 
@@ -553,6 +641,106 @@ std::vector<Seg> segments(MlpState* s, bool grads) {
 }
 
 }  // namespace
+
+// ---------------------------------------------------------------- learned warm start (called by the batch engine)
+// Training set from the answers of the last batched solve, kept on the device:
+// inputs = normalised parameter vectors, targets = normalised [x, y, log(primal
+// weight)] of every instance (external order).  Sets the normalisation.
+int mlp_set_dataset(Ctx* ctx, const float* feat_host, int count, int n, int m, const double* x_dev,
+                    const double* y_dev, const double* om_dev) {
+    MlpState* s = ctx->mlp;
+    if (!s) {
+        ctx->err = "no MLP: call b2p_mlp_create first";
+        return B2P_INVALID_ARGUMENT;
+    }
+    if (s->out != n + m + 1) {
+        ctx->err = "MLP output width must be n + m + 1 of the batch (" + std::to_string(n + m + 1) + ")";
+        return B2P_INVALID_ARGUMENT;
+    }
+    const int in = s->in, out = s->out;
+    cudaStream_t st = ctx->stream;
+    for (auto* d : {&s->in_mean, &s->in_std}) B2P_CUDA(ctx, d->reserve(in));
+    for (auto* d : {&s->out_mean, &s->out_std}) B2P_CUDA(ctx, d->reserve(out));
+    B2P_CUDA(ctx, s->DX.reserve((size_t)count * in));
+    B2P_CUDA(ctx, s->DT.reserve((size_t)count * out));
+    DBuf<float> raw;
+    B2P_CUDA(ctx, raw.reserve((size_t)count * in));
+    B2P_CUDA(ctx, cudaMemcpyAsync(raw.p, feat_host, sizeof(float) * (size_t)count * in, cudaMemcpyHostToDevice, st));
+    k_col_stats<float><<<ew_grid(ctx, in), 256, 0, st>>>(count, in, raw.p, in, 1e-6f, false, s->in_mean.p, s->in_std.p);
+    k_col_stats<double><<<ew_grid(ctx, n), 256, 0, st>>>(count, n, x_dev, n, 1e-4f, false, s->out_mean.p, s->out_std.p);
+    k_col_stats<double><<<ew_grid(ctx, m), 256, 0, st>>>(count, m, y_dev, m, 1e-4f, false, s->out_mean.p + n,
+                                                          s->out_std.p + n);
+    k_col_stats<double><<<1, 32, 0, st>>>(count, 1, om_dev, 1, 1e-4f, true, s->out_mean.p + n + m, s->out_std.p + n + m);
+    // one scale per block (x, y): the root-mean-square of the block's column stds, so
+    // that the squared error in normalised units is the relative L2 error of the
+    // block -- the distance a warm start saves -- and near-constant columns weigh
+    // no more than their share
+    {
+        std::vector<float> sd(out);
+        B2P_CUDA(ctx, cudaMemcpyAsync(sd.data(), s->out_std.p, sizeof(float) * out, cudaMemcpyDeviceToHost, st));
+        B2P_CUDA(ctx, cudaStreamSynchronize(st));
+        for (int blk = 0; blk < 2; ++blk) {
+            const int b0 = blk == 0 ? 0 : n, b1 = blk == 0 ? n : n + m;
+            double q = 0.0;
+            for (int c = b0; c < b1; ++c) q += (double)sd[c] * sd[c];
+            const float rms = (float)std::max(std::sqrt(q / std::max(1, b1 - b0)), 1e-12);
+            for (int c = b0; c < b1; ++c) sd[c] = rms;
+        }
+        B2P_CUDA(ctx, cudaMemcpyAsync(s->out_std.p, sd.data(), sizeof(float) * out, cudaMemcpyHostToDevice, st));
+    }
+    k_norm_rows<<<ew_grid(ctx, (long long)count * in), 256, 0, st>>>(count, in, raw.p, s->in_mean.p, s->in_std.p, s->DX.p);
+    k_build_targets<<<ew_grid(ctx, (long long)count * out), 256, 0, st>>>(count, n, m, x_dev, y_dev, om_dev,
+                                                                        s->out_mean.p, s->out_std.p, s->DT.p);
+    B2P_LAUNCH(ctx);
+    ctx->launches += 6;
+    B2P_CUDA(ctx, cudaStreamSynchronize(st));
+    s->has_norm = true;
+    s->dcount = count;
+    return B2P_OK;
+}
+
+// Warm start of `count` instances of one shape from their parameter vectors:
+// normalise, forward on the tensor cores, de-normalise into x0 [count x n],
+// y0 [count x m] (external order) and primal weights (device, FP64).
+int mlp_predict_warm(Ctx* ctx, const float* feat_host, int count, int n, int m, double* x0, double* y0, double* om) {
+    MlpState* s = ctx->mlp;
+    if (!s || !s->has_norm) {
+        ctx->err = "no trained MLP with normalisation (b2p_mlp_dataset_from_batch or b2p_mlp_set_normalization)";
+        return B2P_INVALID_ARGUMENT;
+    }
+    if (s->out != n + m + 1) {
+        ctx->err = "MLP output width must be n + m + 1 of the batch (" + std::to_string(n + m + 1) + ")";
+        return B2P_INVALID_ARGUMENT;
+    }
+    const int in = s->in;
+    cudaStream_t st = ctx->stream;
+    DBuf<float> raw;
+    B2P_CUDA(ctx, raw.reserve((size_t)count * in));
+    B2P_CUDA(ctx, cudaMemcpyAsync(raw.p, feat_host, sizeof(float) * (size_t)count * in, cudaMemcpyHostToDevice, st));
+    const int chunk = 4096;
+    int r = reserve_batch(ctx, s, std::min(count, chunk));
+    if (r) return r;
+    for (int off = 0; off < count; off += chunk) {
+        const int valid = std::min(chunk, count - off);
+        const int rows = (valid + 7) & ~7;
+        B2P_CUDA(ctx, cudaMemsetAsync(s->Xf.p, 0, sizeof(float) * (size_t)rows * in, st));
+        k_norm_rows<<<ew_grid(ctx, (long long)valid * in), 256, 0, st>>>(valid, in, raw.p + (size_t)off * in,
+                                                                           s->in_mean.p, s->in_std.p, s->Xf.p);
+        k_to_bf16<<<ew_grid(ctx, (long long)rows * in), 256, 0, st>>>(rows, in, s->Xf.p, in, s->Xh.p, in, s->Xt.p, rows);
+        B2P_LAUNCH(ctx);
+        ctx->launches += 2;
+        if ((r = forward(ctx, s, rows, valid, false))) return r;
+        k_out_loss<<<ew_grid(ctx, (long long)rows * s->outp), 256, 0, st>>>(
+            rows, valid, s->out, s->outp, s->G.p, s->b3.p, nullptr, s->Y.p, nullptr, nullptr, 0, nullptr, false);
+        k_denorm_warm<<<ew_grid(ctx, (long long)valid * s->out), 256, 0, st>>>(valid, s->outp, n, m, s->Y.p,
+                                                                              s->out_mean.p, s->out_std.p, off, x0, y0,
+                                                                              om);
+        B2P_LAUNCH(ctx);
+        ctx->launches += 2;
+    }
+    return check_err(ctx, s);
+}
+
 }  // namespace b2p
 
 using namespace b2p;
@@ -717,6 +905,105 @@ int b2p_mlp_gradient(void* p, const float* X, const float* Y, int N, float* loss
         }
         B2P_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     }
+    return B2P_OK;
+}
+
+int b2p_mlp_train(void* p, int epochs, int batch, float lr_start, float lr_end, uint64_t seed, float* loss_out) {
+    Ctx* ctx = static_cast<Ctx*>(p);
+    if (!ctx) return B2P_GPU_UNINITIALIZED;
+    MlpState* s = ctx->mlp;
+    if (!s || s->dcount <= 0 || epochs <= 0 || batch <= 0) {
+        ctx->err = "b2p_mlp_train: no MLP, no device training set, or empty schedule";
+        return B2P_INVALID_ARGUMENT;
+    }
+    cudaSetDevice(ctx->device);
+    const int N = s->dcount, in = s->in, out = s->out;
+    const int b8 = (batch + 7) & ~7;
+    int r = reserve_batch(ctx, s, b8);
+    if (r) return r;
+    B2P_CUDA(ctx, s->perm.reserve(N));
+    cudaStream_t st = ctx->stream;
+    std::vector<int32_t> order(N);
+    std::iota(order.begin(), order.end(), 0);
+    std::mt19937_64 rng(seed);
+    double loss = 0.0;
+    for (int ep = 0; ep < epochs; ++ep) {
+        std::shuffle(order.begin(), order.end(), rng);
+        B2P_CUDA(ctx, cudaMemcpyAsync(s->perm.p, order.data(), sizeof(int32_t) * N, cudaMemcpyHostToDevice, st));
+        const double cosw = 0.5 * (1.0 + std::cos(3.14159265358979323846 * ep / epochs));
+        const float lr = (float)(lr_end + (lr_start - lr_end) * cosw);
+        B2P_CUDA(ctx, cudaMemsetAsync(s->loss.p, 0, sizeof(double), st));
+        for (int off = 0; off < N; off += batch) {
+            const int valid = std::min(batch, N - off);
+            const int rows = (valid + 7) & ~7;
+            k_gather_rows<<<ew_grid(ctx, (long long)rows * in), 256, 0, st>>>(valid, rows, in, s->perm.p + off, s->DX.p,
+                                                                              s->Xf.p);
+            k_gather_rows<<<ew_grid(ctx, (long long)rows * out), 256, 0, st>>>(valid, rows, out, s->perm.p + off,
+                                                                               s->DT.p, s->Tf.p);
+            k_to_bf16<<<ew_grid(ctx, (long long)rows * in), 256, 0, st>>>(rows, in, s->Xf.p, in, s->Xh.p, in, s->Xt.p,
+                                                                           rows);
+            B2P_LAUNCH(ctx);
+            ctx->launches += 3;
+            if ((r = forward(ctx, s, rows, valid, true))) return r;
+            if ((r = backward(ctx, s, rows, valid))) return r;
+            if ((r = adam_step(ctx, s, lr))) return r;
+        }
+        if (ep == epochs - 1) {
+            B2P_CUDA(ctx, cudaMemcpyAsync(&loss, s->loss.p, sizeof(double), cudaMemcpyDeviceToHost, st));
+        }
+        if ((r = check_err(ctx, s))) return r;  // also bounds the queue of launches to one epoch
+    }
+    if (loss_out) *loss_out = (float)(loss / ((double)N * out));
+    return B2P_OK;
+}
+
+int b2p_mlp_get_normalization(void* p, float* in_mean, float* in_std, float* out_mean, float* out_std) {
+    Ctx* ctx = static_cast<Ctx*>(p);
+    if (!ctx) return B2P_GPU_UNINITIALIZED;
+    MlpState* s = ctx->mlp;
+    if (!s || !s->has_norm || !in_mean || !in_std || !out_mean || !out_std) {
+        ctx->err = "b2p_mlp_get_normalization: no normalisation set";
+        return B2P_INVALID_ARGUMENT;
+    }
+    cudaSetDevice(ctx->device);
+    cudaStream_t st = ctx->stream;
+    B2P_CUDA(ctx, cudaMemcpyAsync(in_mean, s->in_mean.p, sizeof(float) * s->in, cudaMemcpyDeviceToHost, st));
+    B2P_CUDA(ctx, cudaMemcpyAsync(in_std, s->in_std.p, sizeof(float) * s->in, cudaMemcpyDeviceToHost, st));
+    B2P_CUDA(ctx, cudaMemcpyAsync(out_mean, s->out_mean.p, sizeof(float) * s->out, cudaMemcpyDeviceToHost, st));
+    B2P_CUDA(ctx, cudaMemcpyAsync(out_std, s->out_std.p, sizeof(float) * s->out, cudaMemcpyDeviceToHost, st));
+    B2P_CUDA(ctx, cudaStreamSynchronize(st));
+    return B2P_OK;
+}
+
+int b2p_mlp_set_normalization(void* p, const float* in_mean, const float* in_std, const float* out_mean,
+                              const float* out_std) {
+    Ctx* ctx = static_cast<Ctx*>(p);
+    if (!ctx) return B2P_GPU_UNINITIALIZED;
+    MlpState* s = ctx->mlp;
+    if (!s || !in_mean || !in_std || !out_mean || !out_std) {
+        ctx->err = "b2p_mlp_set_normalization: no MLP or null argument";
+        return B2P_INVALID_ARGUMENT;
+    }
+    for (int i = 0; i < s->in; ++i)
+        if (!(in_std[i] > 0.0f)) {
+            ctx->err = "b2p_mlp_set_normalization: input std must be positive";
+            return B2P_INVALID_ARGUMENT;
+        }
+    for (int i = 0; i < s->out; ++i)
+        if (!(out_std[i] > 0.0f)) {
+            ctx->err = "b2p_mlp_set_normalization: target std must be positive";
+            return B2P_INVALID_ARGUMENT;
+        }
+    cudaSetDevice(ctx->device);
+    cudaStream_t st = ctx->stream;
+    for (auto* d : {&s->in_mean, &s->in_std}) B2P_CUDA(ctx, d->reserve(s->in));
+    for (auto* d : {&s->out_mean, &s->out_std}) B2P_CUDA(ctx, d->reserve(s->out));
+    B2P_CUDA(ctx, cudaMemcpyAsync(s->in_mean.p, in_mean, sizeof(float) * s->in, cudaMemcpyHostToDevice, st));
+    B2P_CUDA(ctx, cudaMemcpyAsync(s->in_std.p, in_std, sizeof(float) * s->in, cudaMemcpyHostToDevice, st));
+    B2P_CUDA(ctx, cudaMemcpyAsync(s->out_mean.p, out_mean, sizeof(float) * s->out, cudaMemcpyHostToDevice, st));
+    B2P_CUDA(ctx, cudaMemcpyAsync(s->out_std.p, out_std, sizeof(float) * s->out, cudaMemcpyHostToDevice, st));
+    B2P_CUDA(ctx, cudaStreamSynchronize(st));
+    s->has_norm = true;
     return B2P_OK;
 }
 

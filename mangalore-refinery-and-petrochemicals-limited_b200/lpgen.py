@@ -329,3 +329,195 @@ class RefineryFamily:
     def instance(self, p: np.ndarray, name: str = "refinery") -> LP:
         return LP(self.m, self.n, self.rowptr, self.colidx, self.vals, self.sense, self.rhs(p), self.costs(p),
                   np.zeros(self.n), self.ub.copy(), False, name)
+
+
+class RefineryPlanningFamily:
+    """Parametric multi-site refinery planning LP on one fixed structure.
+
+    m = 2000 rows, n = 8000 columns, 6 nonzeros per column on average (seed-fixed):
+
+    * market (192 rows): 96 crude-grade availability rows (<=), each grade contracted
+      to two neighbouring sites (site s buys grades 6s .. 6s+11 mod 96, and the
+      contracted volumes stay below the sites' distillation capacity), and 96
+      (product, region) demand rows (>=), each with an import column (cost 1.5x the
+      base product price: demand is always coverable -> feasible for every
+      parameter vector);
+    * 16 sites of 113 rows / 494 columns each:
+        - 12 crude tanks (=): purchases of the site's 12 grades feed them;
+        - 2 crude distillation units (capacity <=), 3 cut-point modes per (crude,
+          unit): a run draws from the tank and yields 8 cut streams;
+        - 40 stream balances (=): 16 cuts and 24 intermediates;
+        - 12 conversion units (capacity <=), 6 modes each: one feed stream into
+          three product streams (yields summing to 0.95);
+        - 8 product pools: volume balance (=) and 4 linear blending-quality specs
+          (<=: sum over streams of (quality - spec) * volume <= 0);
+        - 7 utility balances (<=, purchasable at a cost) charged by runs and modes;
+        - blending columns (stream -> pool), sales columns (pool -> demand row of 6
+          reachable regions, bounded), stream disposal to fuel;
+    * every column is boxed (0 <= x <= ub): bounded.
+
+    Parameters p in R^256, as a planning department's scenario generator draws
+    them: p[0:64] crude price multipliers U(0.8, 1.2) (grade g -> p[g % 64]),
+    p[64:128] product price multipliers U(0.8, 1.2) ((product, region) pair k ->
+    p[64 + k % 64]), p[128:192] availability scales U(0.7, 1.3) (crude grade g ->
+    p[128 + g % 48], unit capacities -> p[176 + j % 16]), p[192:256] demand scales
+    U(0.7, 1.3) (pair k -> p[192 + k % 64])."""
+
+    N_PARAM = 256
+    SITES, GRADES, PRODUCTS, REGIONS = 16, 96, 8, 12
+    SITE_ROWS, SITE_COLS = 113, 494
+
+    def __init__(self, seed: int = 3):
+        rng = np.random.default_rng(seed)
+        S, G, P, R = self.SITES, self.GRADES, self.PRODUCTS, self.REGIONS
+        K = P * R
+        rows, cols, vals = [], [], []
+        cost, ub = [], []
+        # parameter hooks per column: kind 0 none, 1 crude price, 2 product price
+        cpar_kind, cpar_idx = [], []
+        base_price = np.array([100.0, 95.0, 98.0, 85.0, 60.0, 50.0, 75.0, 90.0])
+        prod_price = base_price[:, None] * rng.uniform(0.95, 1.05, (P, R))  # [P, R]
+        crude_price = rng.uniform(55.0, 75.0, G)
+        self.n_rows_market = G + K
+        m = self.n_rows_market + S * self.SITE_ROWS
+        sense = np.empty(m, np.int32)
+        rhs_base = np.zeros(m)
+        # parameter hooks per row: kind 0 none, 1 availability, 2 capacity, 3 demand
+        rpar_kind = np.zeros(m, np.int32)
+        rpar_idx = np.zeros(m, np.int32)
+        avail_row = np.arange(G)
+        dem_row = G + np.arange(K)
+        sense[avail_row] = LE
+        rhs_base[avail_row] = rng.uniform(20.0, 45.0, G)
+        rpar_kind[avail_row], rpar_idx[avail_row] = 1, np.arange(G) % 48
+        sense[dem_row] = GE
+        rhs_base[dem_row] = rng.uniform(20.0, 60.0, K)
+        rpar_kind[dem_row], rpar_idx[dem_row] = 3, np.arange(K) % 64
+        col = 0
+
+        def add(rlist, vlist, c, u, kind=0, idx=0):
+            nonlocal col
+            rows.append(np.asarray(rlist, np.int64))
+            vals.append(np.asarray(vlist, np.float64))
+            cols.append(np.full(len(rlist), col, np.int64))
+            cost.append(c)
+            ub.append(u)
+            cpar_kind.append(kind)
+            cpar_idx.append(idx)
+            col += 1
+
+        for k in range(K):  # imports, one per demand row
+            add([dem_row[k]], [1.0], 1.5 * base_price[k // R], 1e4)
+        cap_counter = 0
+        for s in range(S):
+            r0 = self.n_rows_market + s * self.SITE_ROWS
+            tank = r0 + np.arange(12)
+            cdu = r0 + 12 + np.arange(2)
+            stream = r0 + 14 + np.arange(40)
+            unit = r0 + 54 + np.arange(12)
+            pool = r0 + 66 + np.arange(P)
+            qual = r0 + 74 + np.arange(P * 4).reshape(P, 4)
+            util = r0 + 106 + np.arange(7)
+            sense[tank] = EQ
+            sense[stream] = EQ
+            sense[pool] = EQ
+            sense[cdu] = LE
+            sense[unit] = LE
+            sense[qual.ravel()] = LE
+            sense[util] = LE
+            rhs_base[cdu] = rng.uniform(250.0, 450.0, 2)
+            rhs_base[unit] = rng.uniform(40.0, 120.0, 12)
+            for r_ in list(cdu) + list(unit):
+                rpar_kind[r_], rpar_idx[r_] = 2, cap_counter % 16
+                cap_counter += 1
+            grades = (s * (G // S) + np.arange(12)) % G  # each grade is contracted to two neighbouring sites
+            regions = rng.choice(R, 6, replace=False)
+            qs = rng.uniform(0.0, 1.0, (40, 4))  # stream qualities
+            spec = rng.uniform(0.35, 0.65, (P, 4))  # product specs
+            for t, g in enumerate(grades):  # purchases
+                add([tank[t], avail_row[g]], [1.0, 1.0], crude_price[g], 1e4, 1, g % 64)
+            for t, g in enumerate(grades):  # distillation runs: (crude, unit, cut-point mode) -> 8 cuts
+                base_y = rng.dirichlet(np.full(8, 2.0))
+                for u in range(2):
+                    for mode in range(3):
+                        y = base_y * rng.uniform(0.8, 1.2, 8)
+                        y = 0.98 * y / y.sum()
+                        uu = rng.choice(7, 2, replace=False)
+                        add([tank[t], cdu[u]] + list(stream[u * 8 + np.arange(8)]) + list(util[uu]),
+                            [-1.0, 1.0] + list(y) + list(rng.uniform(0.01, 0.05, 2)), rng.uniform(0.5, 1.5), 1e3)
+            for j in range(12):  # conversion unit modes: feed -> three intermediates
+                for mode in range(6):
+                    feed = rng.integers(0, 40)
+                    outs = 16 + rng.choice(24, 3, replace=False)
+                    outs = outs[outs != feed][:3]
+                    while len(outs) < 3:
+                        extra = 16 + rng.integers(0, 24)
+                        if extra != feed and extra not in outs:
+                            outs = np.append(outs, extra)
+                    y = rng.dirichlet(np.full(3, 2.0)) * 0.95
+                    uu = rng.choice(7, 2, replace=False)
+                    add([stream[feed], unit[j]] + list(stream[outs]) + list(util[uu]),
+                        [-1.0, 1.0] + list(y) + list(rng.uniform(0.02, 0.1, 2)), rng.uniform(1.0, 5.0), 1e3)
+            for p_ in range(P):  # sales: pool -> reachable regions (bounded), revenue net of transport
+                for r_ in regions:
+                    k = p_ * R + r_
+                    add([pool[p_], dem_row[k]], [-1.0, 1.0], -prod_price[p_, r_] + rng.uniform(1.0, 5.0),
+                        rng.uniform(80.0, 200.0), 2, k % 64)
+            for q in range(40):  # disposal of streams to fuel
+                add([stream[q]], [-1.0], -rng.uniform(20.0, 35.0), 1e3)
+            for q in range(7):  # utility purchase
+                add([util[q]], [-1.0], rng.uniform(5.0, 15.0), 1e3)
+            # blending: the site's remaining columns are (stream -> pool) options
+            n_blend = self.SITE_COLS - (12 + 72 + 72 + P * 6 + 40 + 7)
+            pairs = np.array([(q, p_) for q in range(40) for p_ in range(P)])
+            pick = pairs[np.sort(rng.choice(len(pairs), n_blend, replace=False))]
+            for q, p_ in pick:
+                add([stream[q], pool[p_]] + list(qual[p_]), [-1.0, 1.0] + list(qs[q] - spec[p_]), 0.0, 1e3)
+        n = col
+        rows = np.concatenate(rows)
+        cols = np.concatenate(cols)
+        vals = np.concatenate(vals)
+        self.m, self.n = m, n
+        self.rowptr, self.colidx, self.vals = _csr_from_columns(m, n, rows, cols, vals)
+        self.sense = sense
+        self.rhs_base = rhs_base
+        self.rpar_kind, self.rpar_idx = rpar_kind, rpar_idx
+        self.base_cost = np.asarray(cost)
+        self.cpar_kind = np.asarray(cpar_kind, np.int32)
+        self.cpar_idx = np.asarray(cpar_idx, np.int32)
+        self.ub = np.asarray(ub)
+        self.lb = np.zeros(n)
+
+    def sample_params(self, count: int, seed: int) -> np.ndarray:
+        rng = np.random.default_rng(seed)
+        p = np.empty((count, self.N_PARAM))
+        p[:, :128] = rng.uniform(0.8, 1.2, (count, 128))
+        p[:, 128:] = rng.uniform(0.7, 1.3, (count, 128))
+        return p
+
+    def costs(self, p: np.ndarray) -> np.ndarray:
+        p = np.asarray(p)
+        col = np.where(self.cpar_kind == 1, self.cpar_idx, np.where(self.cpar_kind == 2, 64 + self.cpar_idx, 0))
+        mult = np.where(self.cpar_kind[None, :] > 0, p.reshape(-1, self.N_PARAM)[:, col], 1.0)
+        return (self.base_cost * mult).reshape(p.shape[:-1] + (self.n,))
+
+    def rhs(self, p: np.ndarray) -> np.ndarray:
+        p = np.asarray(p)
+        idx = np.select([self.rpar_kind == 1, self.rpar_kind == 2, self.rpar_kind == 3],
+                        [128 + self.rpar_idx, 176 + self.rpar_idx, 192 + self.rpar_idx], 0)
+        mult = np.where(self.rpar_kind[None, :] > 0, p.reshape(-1, self.N_PARAM)[:, idx], 1.0)
+        return (self.rhs_base * mult).reshape(p.shape[:-1] + (self.m,))
+
+    def instance(self, p: np.ndarray, name: str = "refinery_planning") -> LP:
+        return LP(self.m, self.n, self.rowptr, self.colidx, self.vals, self.sense, self.rhs(p), self.costs(p),
+                  self.lb.copy(), self.ub.copy(), False, name)
+
+    def standard_batch(self, P: np.ndarray):
+        """(shared standard-form matrix as a StdLP of the first instance, B, C, LB, UB, IS_EQ)
+        for parameter vectors P [count x 256]: >= rows negated as in LP.standard()."""
+        P = np.atleast_2d(P)
+        s0 = self.instance(P[0]).standard()
+        mult = np.where(self.sense == GE, -1.0, 1.0)
+        count = P.shape[0]
+        return (s0, self.rhs(P) * mult, self.costs(P), np.tile(self.lb, (count, 1)), np.tile(self.ub, (count, 1)),
+                np.tile(s0.is_eq, (count, 1)))
