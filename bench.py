@@ -1,15 +1,21 @@
 #!/usr/bin/env python
 """LPs/sec to 1e-6 relative KKT on B200 (one JSON line on rank 0).
 
-Default workload: the single large block-angular multi-period blending LP
-(50 period blocks of 4000 x 20000, 8 nnz/col, 4000 inventory-balance rows:
-m = 204,000, n = 1,000,000, nnz ~ 8.0M), solved to 1e-6 relative KKT by the
-mixed-precision Halpern engine (FP32 matrix values and xh gathers, FP64
-iterates / reductions / KKT).  Plain FP64 PDHG on the same LP and GPU is timed
-beside it (`fp64` field).  A "step" is one full solve; N GPUs run N replicas.
+Default workload (refinery_learned): the parametric multi-site refinery planning
+family (fixed 2000 x 8000 structure, 6 nnz/col, 256-dim parameter vector).  Set
+up untimed: 20,000 training instances solved by the batched engine to 1e-8
+relative KKT, the MLP 256 -> 1024 -> 1024 -> 10,001 trained on them on the
+tensor cores.  Timed: 2,000 held-out instances solved to 1e-6 relative KKT by
+(a) learned-warm mixed-precision batched PDHG (the value), (b) cold mixed
+precision, (c) plain FP64 cold start -- same GPU, same instances.  A "step" is
+one batched solve of all held-out instances; N GPUs run N replicas on their own
+held-out seeds (weak scaling).
+
+Other workloads: block_angular (single 204k x 1M LP), random_sparse (300 x 1000),
+uneven_batch (4096 independent LPs), refinery (random-structure family, cold).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                  [--workload block_angular|uneven_batch|refinery|random_sparse]
+                  [--workload refinery_learned|block_angular|uneven_batch|refinery|random_sparse]
 """
 from __future__ import annotations
 
@@ -29,23 +35,28 @@ ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 # Iterations the FP64 Halpern engine needs to reach 1e-6 relative KKT on each
-# workload (measured on B200).  The reference arm's LPs/sec
+# single-LP workload (measured on B200).  The reference arm's LPs/sec
 # extrapolates the reference CPU solver's per-iteration cost over this many
 # iterations -- generous to the CPU: the reference's own vanilla PDHG needs far
 # more iterations and never reaches 1e-6 on these LPs.
-HALPERN_ITERS = {"block_angular": 4928, "random_sparse": 5056}
+HALPERN_ITERS = {"block_angular": 6784, "random_sparse": 5056, "refinery_learned": 67000}
 
 METRIC = "LPs/sec to 1e-6 rel KKT"
+METRIC_LEARNED = "LPs/sec to 1e-6 rel KKT: learned-warm mixed-prec PDHG vs plain FP64, one B200"
 
 
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=None, help="timed steps (default 1 for refinery_learned, else 5)")
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", default="block_angular",
-                    choices=["block_angular", "random_sparse", "uneven_batch", "refinery"])
+    ap.add_argument("--workload", default="refinery_learned",
+                    choices=["refinery_learned", "block_angular", "random_sparse", "uneven_batch", "refinery"])
+    ap.add_argument("--train-count", type=int, default=20000, help="refinery_learned: training instances")
+    ap.add_argument("--label-eps", type=float, default=1e-8, help="refinery_learned: label accuracy")
+    ap.add_argument("--epochs", type=int, default=600, help="refinery_learned: MLP training epochs")
+    ap.add_argument("--heldout", type=int, default=2000, help="refinery_learned: held-out instances per GPU")
     ap.add_argument("--batch-count", type=int, default=4096, help="instances of the batched workloads")
     ap.add_argument("--eps", type=float, default=1e-6)
     ap.add_argument("--no-fp64", action="store_true", help="skip the plain FP64 comparison leg")
@@ -53,7 +64,10 @@ def parse():
     ap.add_argument("--profile", action="store_true",
                     help="profiling case: one short solve, then the two iteration kernels once each inside the "
                          "NVTX range 'kernel_timing' (for ncu --nvtx-include kernel_timing/)")
-    return ap.parse_args()
+    a = ap.parse_args()
+    if a.steps is None:
+        a.steps = 1 if a.workload == "refinery_learned" else 5
+    return a
 
 
 def profile_case(args):
@@ -338,13 +352,212 @@ def run_batch_workload(args):
     ctx.close()
 
 
+def learned_setup(args, rank):
+    """Family, trained warm-start model and held-out parameter vectors of this rank."""
+    import __graft_entry__ as g
+    b2p = g.load_package()
+    fam = b2p.lpgen.RefineryPlanningFamily()
+    P = fam.sample_params(args.heldout, seed=20001 + 1000 * rank)
+    return b2p, fam, P
+
+
+def learned_cfg(args, fam, world):
+    return {"workload": "refinery_planning_learned_warm_start", "m": fam.m, "n": fam.n, "nnz": int(fam.rowptr[-1]),
+            "params": fam.N_PARAM, "train_instances": args.train_count, "label_eps": args.label_eps,
+            "heldout_instances": args.heldout, "mlp": f"{fam.N_PARAM}->1024->1024->{fam.n + fam.m + 1} GELU bf16/fp32acc",
+            "epochs": args.epochs, "eps_rel_kkt": args.eps, "shared_matrix": True, "family_seed": 3,
+            "heldout_seed": 20001, "parallelism": f"replicas x{world}",
+            "l2": "per-instance vectors of 2000 instances (~300 MB) exceed L2; the shared matrix is L2-resident",
+            "warmup": "warm-up steps run the same solves capped at 2048 iterations (autotuning, graphs, allocations)"}
+
+
+def timed_leg(ctx, torch, world, steps, fn):
+    stream = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier(world)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    out = None
+    for _ in range(steps):
+        out = fn()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier(world)
+    return max_over_ranks(e0.elapsed_time(e1), world), out
+
+
+def run_learned_workload(args):
+    import torch
+    rank, world, local = dist_setup(args.gpus)
+    torch.cuda.set_device(local)
+    torch.cuda.set_stream(torch.cuda.Stream())  # CUDA graphs need a non-default stream
+    b2p, fam, P = learned_setup(args, rank)
+    ctx = b2p.Context(local)
+    ctx.set_stream(torch.cuda.current_stream().cuda_stream)
+    ws = b2p.warmstart.LearnedWarmStart(ctx, fam)
+    fit = ws.fit(n_train=args.train_count, label_eps=args.label_eps, epochs=args.epochs)
+    s0 = b2p.warmstart.upload_family(ctx, fam, P)
+    F = P.astype(np.float32)
+    common = dict(eps=args.eps, max_iterations=400000)
+    legs = {
+        "learned": lambda it: ctx.batch_solve_learned(F, fallback=True, precision="fp32", eps=args.eps,
+                                                      max_iterations=it, outputs=False),
+        "mixed_cold": lambda it: ctx.batch_solve(precision="fp32", eps=args.eps, max_iterations=it, outputs=False),
+        "fp64_cold": lambda it: ctx.batch_solve(precision="fp64", eps=args.eps, max_iterations=it, outputs=False),
+    }
+    for _ in range(args.warmup):
+        for fn in legs.values():
+            fn(2048)
+    uuid = None
+    try:
+        uuid = "GPU-" + str(torch.cuda.get_device_properties(local).uuid)
+    except Exception:
+        pass
+    res = {}
+    clocks = None
+    for name, fn in legs.items():
+        sampler = ClockSampler(uuid) if name == "learned" else None
+        if sampler:
+            sampler.start()
+        ms, (summ, per, _, _) = timed_leg(ctx, torch, world, args.steps, lambda: fn(common["max_iterations"]))
+        if sampler:
+            clocks = sampler.stop()
+        solved = sum_over_ranks(float((per["status"] == 0).sum()), world)
+        res[name] = {"value": solved * args.steps / (ms / 1e3), "unit": "LPs/s", "ms_per_step": ms / args.steps,
+                     "solved": int(solved), "instances": args.heldout * world,
+                     "iterations_mean": float(per["iterations"].mean()),
+                     "iterations_max": int(per["iterations"].max()), "worst_rel_kkt": float(per["rel_kkt"].max()),
+                     "kernel_ms": summ["kernel_time_ms"], "kernel_launches": summ["kernel_launches"]}
+        if name == "learned":
+            res[name]["fallbacks"] = summ["fallbacks"]
+            res[name]["warm_used"] = int(per["warm_used"].sum())
+            launches = int(summ["kernel_launches"]) * args.steps
+            it_total = float(per["iterations"].sum())
+            kern_ms = summ["kernel_time_ms"]
+    # end to end through the public API: pinned host parameter vectors and instance
+    # data -> upload -> learned solve -> answers to host
+    _, B, Cc, LB, UB, EQ = fam.standard_batch(P)
+    pin = {k: torch.from_numpy(np.ascontiguousarray(v)).pin_memory()
+           for k, v in (("b", B.ravel()), ("c", Cc.ravel()), ("lb", LB.ravel()), ("ub", UB.ravel()),
+                        ("is_eq", EQ.ravel().astype(np.uint8)), ("f", F))}
+    h2d = sum(t.numel() * t.element_size() for t in pin.values())
+    d2h = 8 * args.heldout * (fam.n + fam.m)
+
+    def e2e_step():
+        ctx.batch_upload([(s0.m, s0.n, s0.rowptr, s0.colidx, s0.vals)], np.zeros(args.heldout, np.int32),
+                         pin["b"].numpy(), pin["c"].numpy(), pin["lb"].numpy(), pin["ub"].numpy(), pin["is_eq"].numpy())
+        return ctx.batch_solve_learned(pin["f"].numpy(), fallback=True, precision="fp32", **common)
+
+    e2e_ms, (esumm, eper, ex, ey) = timed_leg(ctx, torch, world, args.steps, e2e_step)
+    esolved = sum_over_ranks(float((eper["status"] == 0).sum()), world)
+    e2e = {"value": esolved * args.steps / (e2e_ms / 1e3), "unit": "LPs/s", "h2d_bytes_per_step": h2d,
+           "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms / args.steps,
+           "note": "batch upload (host CSR checks, renumbering, device transpose, scaling) + learned solve + x, y"}
+    # roofline of the dominant kernel (k_batch_chunk, FP32): algorithmic bytes of every
+    # instance-iteration of the learned leg over its kernel time
+    nnz = int(fam.rowptr[-1])
+    per_iter = 12 * nnz + 24 * fam.n + 16 * fam.m
+    peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
+    peak = peaks.get("hbm_gbs", 6650.0)
+    achieved = it_total * per_iter / (kern_ms / 1e3) / 1e9
+    traffic = None  # ncu dram read + write of one k_batch_chunk launch / its instance-iterations
+    tfile = ROOT / "profiles" / "batch_chunk_refinery_planning.txt"
+    if tfile.exists():
+        for ln in tfile.read_text().splitlines():
+            if ln.startswith("dram_bytes_per_instance_iteration:"):
+                traffic = float(ln.split(":")[1])
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": traffic, "traffic_unit": "DRAM bytes per instance-iteration (ncu)",
+                "kernel": "k_batch_chunk<float> (SELL-32, learned leg)",
+                "algorithmic_bytes_per_instance_iteration": per_iter,
+                "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if peaks else "fallback 6650 (of fallback)",
+                "note": "12 B per nonzero (FP32 value + 16-bit index, both orientations), 24 B per column, 16 B per "
+                        "row; the shared matrix is served from L2, so DRAM traffic is far below these bytes"}
+    cpu = None
+    if rank == 0 and world == 1:
+        lp0 = fam.instance(P[0])
+        cpu = cpu_reference_sample(lp0, args.cpu_sample_iters * 10, int(res["fp64_cold"]["iterations_mean"]))
+    if rank == 0:
+        ratio = res["learned"]["value"] / res["fp64_cold"]["value"]
+        line = {"metric": METRIC_LEARNED, "value": res["learned"]["value"], "unit": "LPs/s", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": res["learned"]["ms_per_step"],
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f32 (SpMV, vectors) + f64 (scaling, KKT, re-centring); bf16 MLP",
+                "data": "synthetic (seeded refinery planning family, no dataset)",
+                "config": learned_cfg(args, fam, world), "learned_vs_fp64_cold": ratio,
+                "learned": res["learned"], "mixed_cold": res["mixed_cold"], "fp64_cold": res["fp64_cold"],
+                "training": fit, "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "gpu_launches": launches,
+                "clocks": clocks}
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def _ref_worker(q):
+    """One bounded reference CPUFirstOrderSolver sample on the instance of parameter vector q."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import __graft_entry__ as g
+    from oracle_lib import RefLib  # oracle: reference arm only
+    b2p = g.load_package()
+    fam = b2p.lpgen.RefineryPlanningFamily()
+    lp = fam.instance(q)
+    ref = RefLib()
+    r1 = ref.fo_solve(lp, max_iterations=1)
+    r2 = ref.fo_solve(lp, max_iterations=1 + _ref_worker.sample)
+    return r1["solve_time_ms"] / 1e3, (r2["solve_time_ms"] - r1["solve_time_ms"]) / _ref_worker.sample / 1e3
+
+
+_ref_worker.sample = 2000
+
+
+def run_reference_learned(args):
+    """Reference arm of refinery_learned: the reference's CPU PDHG on held-out instances,
+    one instance per host core in parallel; per-LP time = setup + per-iteration cost x
+    the iterations the FP64 engine needs (the reference's own PDHG has no 1e-6 stop
+    rule and does not reach it; extrapolating is generous to the CPU)."""
+    import multiprocessing as mp
+    _, fam, P = learned_setup(args, 0)
+    cores = os.cpu_count() or 1
+    iters = HALPERN_ITERS["refinery_learned"]
+    vals = []
+    t0 = time.perf_counter()
+    with mp.get_context("spawn").Pool(cores) as pool:
+        pool.map(_ref_worker, list(P[:cores]))  # warm-up (loads, page-in)
+        for step in range(args.steps):
+            out = pool.map(_ref_worker, list(P[(step * cores) % len(P):][:cores]))
+            per_lp = [s + it * iters for s, it in out]
+            vals.append(len(out) / max(per_lp))
+    wall = time.perf_counter() - t0
+    v = statistics.median(vals)
+    cb = {"value": v, "unit": "LPs/s", "cores": cores, "kind": "reference",
+          "sample": (f"reference CPUFirstOrderSolver (compiled from its sources), {cores} processes x 1 held-out "
+                     f"instance each: runs of 1 and {1 + _ref_worker.sample} iterations; per-LP time = setup + "
+                     f"{iters} x per-iteration (the FP64 engine's mean iteration count to 1e-6); {wall:.1f} s wall")}
+    line = {"metric": METRIC_LEARNED, "value": v, "unit": "LPs/s", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 / v, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded refinery planning family, no dataset)",
+            "config": learned_cfg(args, fam, 1), "impl": "reference", "cpu_baseline": cb,
+            "e2e": {"value": v, "unit": "LPs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     if args.profile:
         profile_case(args)
         return
     if args.impl == "reference":
-        run_reference(args)
+        if int(os.environ.get("RANK", 0)) != 0:
+            return
+        if args.workload == "refinery_learned":
+            run_reference_learned(args)
+        else:
+            run_reference(args)
+        return
+    if args.workload == "refinery_learned":
+        run_learned_workload(args)
         return
     if args.workload in ("uneven_batch", "refinery"):
         run_batch_workload(args)

@@ -263,10 +263,12 @@ int b2p_mlp_set_normalization(void* ctx, const float* in_mean, const float* in_s
 /* Learned warm start, all on the device: the MLP maps every instance's parameter
  * vector (features: count x in_dim, FP32 host) to x0, y0 and a primal weight, the
  * batch is solved from there (params->precision; default FP32 + re-centring), and
- * with `fallback` != 0 every instance the warm-started run did not solve is
- * solved again from the cold start.  Outputs as b2p_batch_solve, plus
- * warm_used_out[i] = 1 when instance i's answer came from the warm start; the
- * iteration count of a fallen-back instance includes its warm-started run.
+ * with `fallback` != 0 every instance the warm-started run did not solve (a
+ * numerical failure of a bad prediction) is solved again from the cold start with
+ * the iterations left of max_iterations: the count continues, so warm + cold stay
+ * within the cap.  Outputs as b2p_batch_solve, plus warm_used_out[i] = 1 when
+ * instance i's answer came from the warm start; the iteration count of a
+ * fallen-back instance includes its warm-started run.
  * summary->refinement_rounds_done = number of instances that fell back.  Replaces
  * the reference's cold-start-only GPUFirstOrderSolver::solve
  * (src/first_order_solver.cpp:295-306) for parametric families. */

@@ -68,6 +68,7 @@ struct InstCtrl {
     double omega, r0, rprev;
     double rel_p, rel_d, rel_g, pobj, dobj;
     long long k, total, restarts;
+    long long base;  // iterations spent on the instance before this run (cold fallback after a warm run)
     int status, done, first;
     int pad;
 };
@@ -456,7 +457,7 @@ __global__ void __launch_bounds__(512, 2) k_batch_chunk(BArgs a, int chunk) {
                 } else if (sc.rel_p <= a.eps && sc.rel_d <= a.eps && sc.rel_g <= a.eps) {
                     sc.done = 1;
                     sc.status = B2P_STATUS_OPTIMAL;
-                } else if (total >= a.max_iter) {
+                } else if (total + sc.base >= a.max_iter) {
                     sc.done = 1;
                     sc.status = B2P_STATUS_MAX_ITERATIONS;
                 }
@@ -755,7 +756,8 @@ __global__ void k_permute_inst(int count, const int32_t* __restrict__ inst_mat, 
 // centre and the iterates start at 0.
 template <typename MT>
 __global__ void k_batch_init(BArgs a, int count, const int32_t* __restrict__ list, const double* __restrict__ x0,
-                             const double* __restrict__ y0, const double* __restrict__ omega0) {
+                             const double* __restrict__ y0, const double* __restrict__ omega0,
+                             const long long* __restrict__ base0) {
     __shared__ double red[32 * 4];
     ColP<MT>* colp = (ColP<MT>*)a.colp;
     RowP<MT>* rowp = (RowP<MT>*)a.rowp;
@@ -821,6 +823,7 @@ __global__ void k_batch_init(BArgs a, int count, const int32_t* __restrict__ lis
             memset(&s, 0, sizeof(s));
             s.omega = (omega0 && omega0[inst] > 0.0) ? omega0[inst] : ((bn > 1e-10 && cn > 1e-10) ? cn / bn : 1.0);
             s.first = 1;
+            s.base = base0 ? base0[q] : 0;
             s.status = B2P_STATUS_MAX_ITERATIONS;
             a.ictrl[inst] = s;
         }
@@ -971,11 +974,12 @@ size_t smem_bytes(BatchWork* w, size_t mt_size) {
 
 template <typename MT>
 int init_instances(Ctx* ctx, BatchWork* w, const b2p_params* p, const double* x0_dev, const double* y0_dev,
-                   const double* om_dev, const int32_t* list_dev = nullptr, int list_count = 0) {
+                   const double* om_dev, const int32_t* list_dev = nullptr, int list_count = 0,
+                   const long long* base_dev = nullptr) {
     const int cnt = list_dev ? list_count : w->count;
     int grid = std::min(cnt, ctx->sm_count * 8);
     BArgs a = make_args<MT>(w, p, w->active.p);
-    k_batch_init<MT><<<grid, 256, 0, ctx->stream>>>(a, cnt, list_dev, x0_dev, y0_dev, om_dev);
+    k_batch_init<MT><<<grid, 256, 0, ctx->stream>>>(a, cnt, list_dev, x0_dev, y0_dev, om_dev, base_dev);
     B2P_LAUNCH(ctx);
     ctx->launches += 1;
     return B2P_OK;
@@ -1034,7 +1038,7 @@ int autotune(Ctx* ctx, BatchWork* w, const b2p_params* p, TuneCfg* best) {
 template <typename MT>
 int batch_run(Ctx* ctx, BatchWork* w, const b2p_params* p, const double* x0_dev, const double* y0_dev,
               const double* om_dev, const std::vector<int32_t>* subset, bool* timed_out_out, float* kms_out,
-              TuneCfg* cfg_out) {
+              TuneCfg* cfg_out, const std::vector<long long>* base = nullptr) {
     cudaStream_t s = ctx->stream;
     double t_start = now_ms();
     const int64_t IN = w->inst_n, IM = w->inst_m;
@@ -1073,8 +1077,17 @@ int batch_run(Ctx* ctx, BatchWork* w, const b2p_params* p, const double* x0_dev,
         }
         B2P_CUDA(ctx, w->list.reserve(act.size()));
         B2P_CUDA(ctx, cudaMemcpyAsync(w->list.p, act.data(), sizeof(int32_t) * act.size(), cudaMemcpyHostToDevice, s));
-        int st = init_instances<MT>(ctx, w, p, x0_dev, y0_dev, om_dev, w->list.p, (int)act.size());
+        DBuf<long long> dbase;
+        if (base) {  // per listed instance, in list order
+            std::vector<long long> b(act.size());
+            for (size_t q = 0; q < act.size(); ++q) b[q] = (*base)[act[q]];
+            B2P_CUDA(ctx, dbase.reserve(act.size()));
+            B2P_CUDA(ctx, cudaMemcpyAsync(dbase.p, b.data(), sizeof(long long) * b.size(), cudaMemcpyHostToDevice, s));
+        }
+        int st = init_instances<MT>(ctx, w, p, x0_dev, y0_dev, om_dev, w->list.p, (int)act.size(),
+                                    base ? dbase.p : nullptr);
         if (st) return st;
+        B2P_CUDA(ctx, cudaStreamSynchronize(s));  // dbase is released at scope end
     } else {
         act = w->order;
         int st = init_instances<MT>(ctx, w, p, x0_dev, y0_dev, om_dev);
@@ -1178,11 +1191,11 @@ int collect_outputs(Ctx* ctx, BatchWork* w, bool timed_out, int32_t* status_out,
         int stt = c.done ? c.status : (timed_out ? B2P_STATUS_INTERRUPTED : B2P_STATUS_MAX_ITERATIONS);
         double kk = std::max(c.rel_p, std::max(c.rel_d, c.rel_g));
         if (status_out) status_out[i] = stt;
-        if (iters_out) iters_out[i] = c.total;
+        if (iters_out) iters_out[i] = c.total + c.base;
         if (kkt_out) kkt_out[i] = kk;
         if (omega_out) omega_out[i] = c.omega;
-        *tot_it += c.total;
-        *maxit = std::max<int64_t>(*maxit, c.total);
+        *tot_it += c.total + c.base;
+        *maxit = std::max<int64_t>(*maxit, c.total + c.base);
         *opt += (stt == B2P_STATUS_OPTIMAL);
         *worst = std::max(*worst, kk);
     }
@@ -1570,36 +1583,35 @@ int b2p_batch_solve_learned(void* p, const b2p_params* params, const float* feat
     st = f64 ? batch_run<double>(ctx, w, pp, dx0.p, dy0.p, dom.p, nullptr, &timed_out, &kms, &cfg)
              : batch_run<float>(ctx, w, pp, dx0.p, dy0.p, dom.p, nullptr, &timed_out, &kms, &cfg);
     if (st) return st;
-    // cold-start fallback for every instance the warm-started run did not solve
-    std::vector<int64_t> warm_iters(w->count);
+    // cold-start fallback for every instance the warm-started run did not solve and
+    // that has iterations left: the cold run continues the instance's iteration count,
+    // so warm + cold together stay within max_iterations (an instance that spent its
+    // whole budget warm is reported MAX_ITERATIONS, as a cold run would be)
+    std::vector<long long> warm_iters(w->count);
     std::vector<int32_t> failed;
     for (int i = 0; i < w->count; ++i) {
         warm_iters[i] = w->hc[i].total;
-        if (!(w->hc[i].done && w->hc[i].status == B2P_STATUS_OPTIMAL)) failed.push_back(i);
+        const bool ok = w->hc[i].done && w->hc[i].status == B2P_STATUS_OPTIMAL;
+        if (!ok && warm_iters[i] < pp->max_iterations) failed.push_back(i);
     }
     if (fallback && !failed.empty() && !timed_out) {
-        st = f64 ? batch_run<double>(ctx, w, pp, nullptr, nullptr, nullptr, &failed, &timed_out, &kms2, &cfg)
-                 : batch_run<float>(ctx, w, pp, nullptr, nullptr, nullptr, &failed, &timed_out, &kms2, &cfg);
+        st = f64 ? batch_run<double>(ctx, w, pp, nullptr, nullptr, nullptr, &failed, &timed_out, &kms2, &cfg,
+                                     &warm_iters)
+                 : batch_run<float>(ctx, w, pp, nullptr, nullptr, nullptr, &failed, &timed_out, &kms2, &cfg,
+                                    &warm_iters);
         if (st) return st;
     }
     int64_t tot_it, maxit, opt;
     double worst;
-    st = collect_outputs(ctx, w, timed_out, status_out, nullptr, kkt_out, nullptr, x_out, y_out, &tot_it, &maxit, &opt,
-                         &worst);
+    // iterations per instance: the warm run, plus the cold run when it fell back
+    st = collect_outputs(ctx, w, timed_out, status_out, iters_out, kkt_out, nullptr, x_out, y_out, &tot_it, &maxit,
+                         &opt, &worst);
     if (st) return st;
     std::vector<uint8_t> is_failed(w->count, 0);
     if (fallback)
         for (int32_t i : failed) is_failed[i] = 1;
-    tot_it = 0;
-    maxit = 0;
-    for (int i = 0; i < w->count; ++i) {
-        // iterations spent on the instance: the warm run, plus the cold run when it fell back
-        const int64_t it = is_failed[i] ? warm_iters[i] + w->hc[i].total : w->hc[i].total;
-        if (iters_out) iters_out[i] = it;
-        if (warm_used_out) warm_used_out[i] = is_failed[i] ? 0 : 1;
-        tot_it += it;
-        maxit = std::max(maxit, it);
-    }
+    if (warm_used_out)
+        for (int i = 0; i < w->count; ++i) warm_used_out[i] = is_failed[i] ? 0 : 1;
     fill_summary(summary, w->count, timed_out, tot_it, maxit, opt, worst, kms + kms2, cfg);
     if (summary) {
         summary->solve_time_ms = now_ms() - t0;

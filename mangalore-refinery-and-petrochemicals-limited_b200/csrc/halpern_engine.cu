@@ -25,7 +25,7 @@
 // one-thread control kernel, so a chunk is a fixed kernel sequence that is
 // captured once as a CUDA graph and replayed until the control block says done.
 //
-// Kernels per iteration (HBM-bound; see DESIGN.md for the byte counts):
+// Kernels per iteration (HBM-bound; algorithmic bytes in kernel_timing_T below):
 //   k_primal : A^T y (CSR of A^T, L lanes per column) + projected primal step
 //              + extrapolation + Halpern update (+ check reductions)
 //   k_dual   : A xh  (CSR of A,   L lanes per row)    + projected dual step

@@ -309,12 +309,14 @@ class RefineryFamily:
         self.av_group = np.arange(n_av) % 64
         self.dem_group = np.arange(n_dem) % 64
 
-    def sample_params(self, count: int, seed: int) -> np.ndarray:
+    def sample_params(self, count: int, seed: int, spread: float = 1.0) -> np.ndarray:
+        """Price multipliers U(0.8, 1.2), rhs scales U(0.7, 1.3); `spread` < 1 narrows
+        both ranges around 1 (a family whose solution map is nearly linear)."""
         rng = np.random.default_rng(seed)
         p = np.empty((count, self.N_PARAM))
         p[:, :128] = rng.uniform(0.8, 1.2, (count, 128))
         p[:, 128:] = rng.uniform(0.7, 1.3, (count, 128))
-        return p
+        return 1.0 + spread * (p - 1.0)
 
     def costs(self, p: np.ndarray) -> np.ndarray:
         mult = np.where(self.price_group >= 0, p[..., np.maximum(self.price_group, 0)], 1.0)
@@ -329,6 +331,16 @@ class RefineryFamily:
     def instance(self, p: np.ndarray, name: str = "refinery") -> LP:
         return LP(self.m, self.n, self.rowptr, self.colidx, self.vals, self.sense, self.rhs(p), self.costs(p),
                   np.zeros(self.n), self.ub.copy(), False, name)
+
+    def standard_batch(self, P: np.ndarray):
+        """(shared standard-form matrix as a StdLP of the first instance, B, C, LB, UB, IS_EQ)
+        for parameter vectors P [count x 256]: >= rows negated as in LP.standard()."""
+        P = np.atleast_2d(P)
+        s0 = self.instance(P[0]).standard()
+        mult = np.where(self.sense == GE, -1.0, 1.0)
+        count = P.shape[0]
+        return (s0, self.rhs(P) * mult, self.costs(P), np.zeros((count, self.n)), np.tile(self.ub, (count, 1)),
+                np.tile(s0.is_eq, (count, 1)))
 
 
 class RefineryPlanningFamily:
@@ -488,12 +500,14 @@ class RefineryPlanningFamily:
         self.ub = np.asarray(ub)
         self.lb = np.zeros(n)
 
-    def sample_params(self, count: int, seed: int) -> np.ndarray:
+    def sample_params(self, count: int, seed: int, spread: float = 1.0) -> np.ndarray:
+        """Price multipliers U(0.8, 1.2), rhs scales U(0.7, 1.3); `spread` < 1 narrows
+        both ranges around 1 (a family whose solution map is nearly linear)."""
         rng = np.random.default_rng(seed)
         p = np.empty((count, self.N_PARAM))
         p[:, :128] = rng.uniform(0.8, 1.2, (count, 128))
         p[:, 128:] = rng.uniform(0.7, 1.3, (count, 128))
-        return p
+        return 1.0 + spread * (p - 1.0)
 
     def costs(self, p: np.ndarray) -> np.ndarray:
         p = np.asarray(p)
