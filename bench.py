@@ -70,6 +70,42 @@ def parse():
     return a
 
 
+def profile_learned(args):
+    """Profiling case of refinery_learned (for ncu, NVTX range 'timed'): a small
+    training run (1024 labels to 1e-6, 20 epochs), then the three legs on 1024
+    held-out instances capped at 100k iterations -- per-instance vectors of the
+    held-out batch (~240 MB) exceed L2 like the full workload's."""
+    import torch
+    torch.cuda.set_device(0)
+    torch.cuda.set_stream(torch.cuda.Stream())
+    b2p, fam, _ = learned_setup(args, 0)
+    P = fam.sample_params(1024, seed=20001)
+    with b2p.Context(0) as ctx:
+        ctx.set_stream(torch.cuda.current_stream().cuda_stream)
+        ws = b2p.warmstart.LearnedWarmStart(ctx, fam)
+        ws.fit(n_train=1024, label_eps=1e-6, epochs=20, max_iterations=100000)
+        b2p.warmstart.upload_family(ctx, fam, P)
+        F = P.astype(np.float32)
+        legs = {
+            "learned": lambda it: ctx.batch_solve_learned(F, precision="fp32", eps=args.eps, max_iterations=it,
+                                                          outputs=False),
+            "mixed_cold": lambda it: ctx.batch_solve(precision="fp32", eps=args.eps, max_iterations=it, outputs=False),
+            "fp64_cold": lambda it: ctx.batch_solve(precision="fp64", eps=args.eps, max_iterations=it, outputs=False),
+        }
+        for fn in legs.values():
+            fn(2048)
+        torch.cuda.synchronize()
+        torch.cuda.nvtx.range_push("timed")
+        out = {}
+        for name, fn in legs.items():
+            summ, per, _, _ = fn(100000)
+            out[name] = {"kernel_ms": summ["kernel_time_ms"], "iterations_mean": float(per["iterations"].mean()),
+                         "instance_iterations": int(per["iterations"].sum()), "launches": summ["kernel_launches"]}
+        torch.cuda.synchronize()
+        torch.cuda.nvtx.range_pop()
+        print(json.dumps(out), flush=True)
+
+
 def profile_case(args):
     import torch
     torch.cuda.set_device(0)
@@ -546,7 +582,7 @@ def run_reference_learned(args):
 def main():
     args = parse()
     if args.profile:
-        profile_case(args)
+        profile_learned(args) if args.workload == "refinery_learned" else profile_case(args)
         return
     if args.impl == "reference":
         if int(os.environ.get("RANK", 0)) != 0:
