@@ -202,24 +202,26 @@ def barrier(world):
         dist.barrier()
 
 
-def max_over_ranks(v, world):
+def _reduce(v, world, op):
     if world == 1:
         return v
     import torch
     import torch.distributed as dist
-    t = torch.tensor([v], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    dev = "cpu" if dist.get_backend() == "gloo" else "cuda"
+    t = torch.tensor([v], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=op)
     return float(t.item())
+
+
+def max_over_ranks(v, world):
+    """Slowest rank's time: the whole job's time (one scalar all-reduce)."""
+    import torch.distributed as dist
+    return _reduce(v, world, dist.ReduceOp.MAX if world > 1 else None)
 
 
 def sum_over_ranks(v, world):
-    if world == 1:
-        return v
-    import torch
     import torch.distributed as dist
-    t = torch.tensor([v], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.SUM)
-    return float(t.item())
+    return _reduce(v, world, dist.ReduceOp.SUM if world > 1 else None)
 
 
 def timed_solves(ctx, torch, steps, world, **params):
