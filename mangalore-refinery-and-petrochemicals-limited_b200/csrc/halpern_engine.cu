@@ -327,28 +327,44 @@ __global__ void __launch_bounds__(1024) k_iter(IterArgs<VT, GT> a, int it) {
             k0[u] = v ? ld_stream(a.ptr + r[u], pol) : 0;
             k1[u] = v ? ld_stream(a.ptr + r[u] + 1, pol) : 0;
         }
-        double zr[R], cst[R];
+        // the row's own vectors, prefetched with the row pointers (they are only needed
+        // after the reduction, so their latency overlaps the matrix stream)
+        double zr[R], cst[R], lo[R], hi[R], zan[R];
 #pragma unroll
         for (int u = 0; u < R; ++u) {
             const bool lead = sub == 0 && r[u] < row1;
             zr[u] = lead ? a.z[r[u]] : 0.0;
             cst[u] = lead ? a.cost[r[u]] : 0.0;
+            zan[u] = lead ? a.za[r[u]] : 0.0;
+            if (PRIMAL) {
+                lo[u] = lead ? a.lo[r[u]] : 0.0;
+                hi[u] = lead ? a.hi[r[u]] : 0.0;
+            } else {
+                lo[u] = (lead && !a.is_eq[r[u]]) ? (a.ylb ? a.ylb[r[u]] : 0.0) : -INFINITY;
+                hi[u] = 0.0;
+            }
         }
-        VT v[R];
-        int c[R];
-#pragma unroll
-        for (int u = 0; u < R; ++u) {
-            const int k = k0[u] + sub;
-            const bool h = k < k1[u];
-            v[u] = h ? ld_stream(a.val + k, pol) : (VT)0;
-            c[u] = h ? ld_stream(a.idx + k, pol) : -1;
-        }
-        double s[R];
-#pragma unroll
-        for (int u = 0; u < R; ++u) s[u] = (c[u] >= 0) ? (double)v[u] * (double)a.gather[c[u]] : 0.0;
+        // the first two entries of every lane, all loads in flight together
+        VT v[R][2];
+        int c[R][2];
 #pragma unroll
         for (int u = 0; u < R; ++u)
-            for (int k = k0[u] + sub + L; k < k1[u]; k += L)
+#pragma unroll
+            for (int e = 0; e < 2; ++e) {
+                const int k = k0[u] + sub + e * L;
+                const bool h = k < k1[u];
+                v[u][e] = h ? ld_stream(a.val + k, pol) : (VT)0;
+                c[u][e] = h ? ld_stream(a.idx + k, pol) : -1;
+            }
+        double s[R];
+#pragma unroll
+        for (int u = 0; u < R; ++u) {
+            s[u] = (c[u][0] >= 0) ? (double)v[u][0] * (double)a.gather[c[u][0]] : 0.0;
+            if (c[u][1] >= 0) s[u] += (double)v[u][1] * (double)a.gather[c[u][1]];
+        }
+#pragma unroll
+        for (int u = 0; u < R; ++u)
+            for (int k = k0[u] + sub + 2 * L; k < k1[u]; k += L)
                 s[u] += (double)ld_stream(a.val + k, pol) * (double)a.gather[ld_stream(a.idx + k, pol)];
 #pragma unroll
         for (int u = 0; u < R; ++u) {
@@ -361,16 +377,13 @@ __global__ void __launch_bounds__(1024) k_iter(IterArgs<VT, GT> a, int it) {
             const int row = r[u];
             double zt;
             if (PRIMAL) {
-                zt = clampT(zr[u] - step * (cst[u] + s[u]), a.lo[row], a.hi[row]);
+                zt = clampT(zr[u] - step * (cst[u] + s[u]), lo[u], hi[u]);
                 a.zh[row] = (VT)(2.0 * zt - zr[u]);
             } else {
                 zt = zr[u] + step * (s[u] - cst[u]);
-                if (!a.is_eq[row]) {
-                    const double lbv = a.ylb ? a.ylb[row] : 0.0;
-                    if (zt < lbv) zt = lbv;
-                }
+                if (zt < lo[u]) zt = lo[u];  // -inf on equality rows; NaN stays NaN
             }
-            const double za = a.za[row];
+            const double za = zan[u];
             a.z[row] = wk * ((1.0 + rho) * zt - rho * zr[u]) + wa * za;
             if (MODE != M_PLAIN) {
                 const double d = zr[u] - zt;
