@@ -66,6 +66,9 @@ def highs_lps():
         out[f"batch12_{i}"] = lp
     fam = lpgen.RefineryFamily()
     out["refinery_p0"] = fam.instance(fam.sample_params(1, 0)[0])
+    plan = lpgen.RefineryPlanningFamily()
+    for i, q in enumerate(plan.sample_params(3, 20001)):  # the first held-out instances of the benchmark
+        out[f"planning_heldout_{i}"] = plan.instance(q)
     return out
 
 

@@ -113,3 +113,20 @@ def test_batch_rejects_bad_input(ctx, b2p):
         ctx.batch_upload([(1, 2, rp, ci, np.ones(2))], np.zeros(1, np.int32), np.ones(1), np.ones(2), np.zeros(2),
                          np.ones(2), np.zeros(1, np.uint8))
     assert e.value.code == b2p.INVALID_ARGUMENT
+
+
+def test_planning_family_matches_highs(ctx, golden, lpgen, b2p):
+    """The first held-out instances of the benchmark's refinery planning family:
+    mixed-precision batched answers reach the HiGHS optimum to 1e-6 relative."""
+    fam = lpgen.RefineryPlanningFamily()
+    P = fam.sample_params(3, 20001)
+    s0, B, Cc, LB, UB, EQ = fam.standard_batch(P)
+    b2p.warmstart.upload_family(ctx, fam, P)
+    _, per, x, y = ctx.batch_solve(precision="fp32", eps=1e-7, max_iterations=400000)
+    assert np.all(per["status"] == 0), per
+    for i in range(3):
+        s = lpgen.StdLP(s0.m, s0.n, s0.rowptr, s0.colidx, s0.vals, B[i], Cc[i], LB[i], UB[i], EQ[i])
+        k = pdlp_oracle.kkt(s, x[i * fam.n:(i + 1) * fam.n], y[i * fam.m:(i + 1) * fam.m])
+        assert k["rel_kkt"] <= 1.05e-7, (i, k)
+        z = golden["highs"][f"planning_heldout_{i}"]
+        assert abs(k["pobj"] - z) <= 1e-6 * max(1.0, abs(z)), (i, k["pobj"], z)
