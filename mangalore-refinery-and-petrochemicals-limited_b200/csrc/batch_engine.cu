@@ -1043,6 +1043,19 @@ int batch_run(Ctx* ctx, BatchWork* w, const b2p_params* p, const double* x0_dev,
     double t_start = now_ms();
     const int64_t IN = w->inst_n, IM = w->inst_m;
     const int prec = sizeof(MT) == 8 ? 0 : 1;
+    {
+        // y and xh of the largest instance must fit one CTA's shared memory
+        int max_smem = 0;
+        B2P_CUDA(ctx, cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->device));
+        const size_t need = smem_bytes(w, sizeof(MT));
+        if (need > (size_t)max_smem) {
+            ctx->err = "batch instance too large for one CTA's shared memory: needs " + std::to_string(need) +
+                       " bytes (" + std::to_string(w->max_m) + " rows + " + std::to_string(w->max_n) +
+                       " columns), the device allows " + std::to_string(max_smem) +
+                       "; solve it with b2p_solve";
+            return B2P_INVALID_ARGUMENT;
+        }
+    }
     w->recenter = false;  // autotune trials run without re-centring
     TuneCfg cfg = {256, 2048};
     if (w->tuned_threads[prec] > 0) {
