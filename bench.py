@@ -42,6 +42,10 @@ sys.path.insert(0, str(ROOT))
 HALPERN_ITERS = {"block_angular": 6784, "random_sparse": 5056, "refinery_learned": 65388}
 
 METRIC = "LPs/sec to 1e-6 rel KKT"
+
+
+def metric_for(args):
+    return f"LPs/sec to {args.eps:g} rel KKT"
 METRIC_LEARNED = "LPs/sec to 1e-6 rel KKT: learned-warm mixed-prec PDHG vs plain FP64, one B200"
 
 
@@ -52,13 +56,15 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", default="refinery_learned",
-                    choices=["refinery_learned", "block_angular", "random_sparse", "uneven_batch", "refinery"])
+                    choices=["refinery_learned", "block_angular", "random_sparse", "uneven_batch", "refinery",
+                             "ill_conditioned"])
     ap.add_argument("--train-count", type=int, default=20000, help="refinery_learned: training instances")
     ap.add_argument("--label-eps", type=float, default=1e-8, help="refinery_learned: label accuracy")
     ap.add_argument("--epochs", type=int, default=600, help="refinery_learned: MLP training epochs")
     ap.add_argument("--heldout", type=int, default=2000, help="refinery_learned: held-out instances per GPU")
     ap.add_argument("--batch-count", type=int, default=4096, help="instances of the batched workloads")
-    ap.add_argument("--eps", type=float, default=1e-6)
+    ap.add_argument("--eps", type=float, default=None,
+                    help="relative KKT tolerance (default 1e-8 for ill_conditioned, else 1e-6)")
     ap.add_argument("--no-fp64", action="store_true", help="skip the plain FP64 comparison leg")
     ap.add_argument("--cpu-sample-iters", type=int, default=20)
     ap.add_argument("--profile", action="store_true",
@@ -66,7 +72,9 @@ def parse():
                          "NVTX range 'kernel_timing' (for ncu --nvtx-include kernel_timing/)")
     a = ap.parse_args()
     if a.steps is None:
-        a.steps = 1 if a.workload == "refinery_learned" else 5
+        a.steps = 1 if a.workload in ("refinery_learned", "ill_conditioned") else 5
+    if a.eps is None:
+        a.eps = 1e-8 if a.workload == "ill_conditioned" else 1e-6
     return a
 
 
@@ -129,6 +137,10 @@ def make_lp(workload):
         lp = b2p.lpgen.block_angular()
         cfg = {"workload": "block_angular_multiperiod_blending", "m": lp.m, "n": lp.n, "nnz": lp.nnz,
                "periods": 50, "block": "4000x20000", "nnz_per_col": 8, "link_rows": 4000, "seed": 1}
+    elif workload == "ill_conditioned":
+        lp = b2p.lpgen.ill_conditioned()
+        cfg = {"workload": "ill_conditioned_stress", "m": lp.m, "n": lp.n, "nnz": lp.nnz, "nnz_per_col": 10,
+               "row_scales": "10^U(-4,4)", "col_scales": "10^U(-3,3)", "box": "[0, 10^U(0,3)]", "seed": 4}
     else:
         lp = b2p.lpgen.random_sparse()
         cfg = {"workload": "random_sparse_300x1000", "m": lp.m, "n": lp.n, "nnz": lp.nnz, "seed": 0}
@@ -301,7 +313,7 @@ def run_reference(args):
     v = statistics.median([c["value"] for c in vals])
     cb = dict(vals[-1])
     cb["value"] = v
-    line = {"metric": METRIC, "value": v, "unit": "LPs/s", "n_gpus": args.gpus, "steps": args.steps,
+    line = {"metric": metric_for(args), "value": v, "unit": "LPs/s", "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1e3 / v, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator, no dataset)",
             "config": cfg, "impl": "reference", "cpu_baseline": cb,
@@ -379,7 +391,7 @@ def run_batch_workload(args):
     peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
     peak = peaks.get("hbm_gbs", 6650.0)
     achieved = alg / (res["fp32"]["ms_per_step"] / 1e3) / 1e9
-    line = {"metric": METRIC, "value": res["fp32"]["value"], "unit": "LPs/s", "n_gpus": 1, "steps": args.steps,
+    line = {"metric": metric_for(args), "value": res["fp32"]["value"], "unit": "LPs/s", "n_gpus": 1, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": res["fp32"]["ms_per_step"], "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32 values + f64 iterates/KKT",
             "data": "synthetic (seeded generator, no dataset)", "config": cfg, "mixed": res["fp32"], "fp64": res["fp64"],
@@ -614,10 +626,12 @@ def main():
     ctx = b2p.Context(local)
     ctx.set_stream(torch.cuda.current_stream().cuda_stream)
     ctx.upload(std)
-    common = dict(engine="halpern", eps=args.eps, max_iterations=1_000_000)
-    # warm-up (also fills the autotune / allocation caches)
+    common = dict(engine="halpern", eps=args.eps, max_iterations=2_000_000)
+    # warm-up (also fills the autotune / allocation caches); on the stress LP, whose
+    # solve takes minutes, warm-up solves stop after 4096 iterations
+    warm = dict(common, max_iterations=4096) if args.workload == "ill_conditioned" else common
     for _ in range(args.warmup):
-        ctx.solve(precision="fp32", **common)
+        ctx.solve(precision="fp32", **warm)
     uuid = None
     try:
         uuid = "GPU-" + str(torch.cuda.get_device_properties(local).uuid)
@@ -636,7 +650,7 @@ def main():
     fp64 = None
     if not args.no_fp64:
         for _ in range(1):
-            ctx.solve(precision="fp64", **common)
+            ctx.solve(precision="fp64", **warm)
         ms64, res64 = timed_solves(ctx, torch, args.steps, world, precision="fp64", **common)
         ms64 = max_over_ranks(ms64, world)
         fp64 = {"value": (args.steps * world) / (ms64 / 1e3), "unit": "LPs/s", "iterations": res64[-1]["iterations"],
@@ -698,12 +712,13 @@ def main():
     if rank == 0 and world == 1:
         cpu = cpu_reference_sample(lp, args.cpu_sample_iters, fp64["iterations"] if fp64 else iters)
     if rank == 0:
-        line = {"metric": METRIC, "value": value, "unit": "LPs/s", "n_gpus": world, "steps": args.steps,
+        line = {"metric": metric_for(args), "value": value, "unit": "LPs/s", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32 values + f64 iterates/KKT",
                 "data": "synthetic (seeded generator, no dataset)",
                 "config": dict(cfg, parallelism=f"replicas x{world}", eps_rel_kkt=args.eps,
-                               l2="inputs larger than L2 (scaled A and A^T: ~390 MB)", engine="halpern/mixed"),
+                               l2=f"inputs larger than L2 (scaled A and A^T: ~{16 * lp.nnz / 1e6:.0f} MB)",
+                               engine="halpern/mixed"),
                 "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "gpu_launches": launches,
                 "clocks": clocks, "iterations": iters, "solved": int(solved), "fp64": fp64,
                 "rel_kkt": results[-1]["rel_kkt"]}

@@ -583,6 +583,7 @@ int b2p_upload_lp(void* p, int m, int n, int64_t nnz, const int32_t* rowptr, con
     int mr = 0;
     for (int i = 0; i < m; ++i) mr = std::max(mr, rowptr[i + 1] - rowptr[i]);
     L.max_row_len = mr;
+    ctx->lp_gen += 1;
     ctx->has_lp = true;
     return B2P_OK;
 }

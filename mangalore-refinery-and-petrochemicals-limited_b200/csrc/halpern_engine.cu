@@ -30,6 +30,8 @@
 //              + extrapolation + Halpern update (+ check reductions)
 //   k_dual   : A xh  (CSR of A,   L lanes per row)    + projected dual step
 //              + Halpern update (+ check reductions)
+#include <cub/cub.cuh>
+
 #include <cmath>
 #include <cstring>
 #include <algorithm>
@@ -63,8 +65,35 @@ struct Ctrl {
 // private status of a solve that reached its inner tolerance (refinement continues)
 constexpr int kInnerDone = 100;
 
+// SELL-32 copy of one orientation of the scaled matrix (internal numbering): slice s
+// holds rows 32s..32s+31; its entries are stored in chunks of W per lane -- entry e
+// of lane l sits at off[s] + (e / W) * 32 W + l W + e % W -- so one warp-wide
+// load of W consecutive elements per lane reads 32 W contiguous elements.  Rows
+// shorter than the slice's longest are zero-padded (value 0, index 0).
+struct Sell {
+    int W = 1;
+    int64_t slices = 0, total = 0;
+    DBuf<int64_t> off;   // slices + 1
+    DBuf<int32_t> idx;   // total
+    DBuf<float> v32;     // total (mixed engine)
+    DBuf<double> v64;    // total (FP64 engine)
+    bool idx_ready = false;
+};
+
 struct HalpernWork {
     int m = -1, n = -1;
+    // Internal numbering: rows and columns sorted by decreasing length inside
+    // windows of kWindow, so that each 32-row slice of the SELL copies is nearly
+    // uniform while neighbouring rows stay neighbours.  The engine works on `ilp`,
+    // the uploaded LP renumbered; warm starts and answers are permuted on the device.
+    int64_t ilp_gen = -1;        // ctx->lp_gen the internal copy was built from
+    DevLP ilp;
+    DBuf<int32_t> pr, pc;        // internal -> original row / column
+    DBuf<int32_t> ic, ir;        // original -> internal column / row
+    Sell sr, sc;                 // SELL copies of A (rows) and A^T (columns)
+    bool sell_r = false, sell_c = false;  // tuned: SELL (true) or CSR kernel per side
+    int64_t solved_gen = -1;     // upload generation and precision of the last solve
+    int solved_precision = -1;   // (the state b2p_kernel_timing replays)
     DBuf<double> dr, dc, tmp_m, tmp_n, pv, pu, pw;
     DBuf<double> sv64, stv64;      // scaled A and A^T, FP64 (KKT, power iteration, FP64 engine)
     DBuf<float> sv32, stv32;       // scaled A and A^T, FP32 (FP32 engine)
@@ -261,6 +290,7 @@ struct IterArgs {
     Ctrl* ctrl;
     int rows;
     double rho;
+    const int64_t* soff;   // SELL kernel: slice offsets (ptr / idx / val unused by it except idx, val)
 };
 
 // Matrix entries and row pointers are read once per iteration: bypass L1 and mark
@@ -285,6 +315,48 @@ __device__ __forceinline__ int ld_stream(const int* p, unsigned long long pol) {
     int v;
     asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.s32 %0, [%1], %2;" : "=r"(v) : "l"(p), "l"(pol));
     return v;
+}
+__device__ __forceinline__ long long ld_stream(const long long* p, unsigned long long pol) {
+    long long v;
+    asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.s64 %0, [%1], %2;" : "=l"(v) : "l"(p), "l"(pol));
+    return v;
+}
+
+// W consecutive elements (W * sizeof(T) aligned) in one or two vector loads, streaming policy.
+template <int W>
+__device__ __forceinline__ void ld_stream_w(const float* p, float (&v)[W], unsigned long long pol) {
+    if constexpr (W == 4) {
+        asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.v4.f32 {%0,%1,%2,%3}, [%4], %5;"
+                     : "=f"(v[0]), "=f"(v[1]), "=f"(v[2]), "=f"(v[3]) : "l"(p), "l"(pol));
+    } else if constexpr (W == 2) {
+        asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.v2.f32 {%0,%1}, [%2], %3;"
+                     : "=f"(v[0]), "=f"(v[1]) : "l"(p), "l"(pol));
+    } else {
+        v[0] = ld_stream(p, pol);
+    }
+}
+template <int W>
+__device__ __forceinline__ void ld_stream_w(const double* p, double (&v)[W], unsigned long long pol) {
+    if constexpr (W >= 2) {
+#pragma unroll
+        for (int h = 0; h < W; h += 2)
+            asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.v2.f64 {%0,%1}, [%2], %3;"
+                         : "=d"(v[h]), "=d"(v[h + 1]) : "l"(p + h), "l"(pol));
+    } else {
+        v[0] = ld_stream(p, pol);
+    }
+}
+template <int W>
+__device__ __forceinline__ void ld_stream_w(const int* p, int (&v)[W], unsigned long long pol) {
+    if constexpr (W == 4) {
+        asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.v4.s32 {%0,%1,%2,%3}, [%4], %5;"
+                     : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]) : "l"(p), "l"(pol));
+    } else if constexpr (W == 2) {
+        asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.v2.s32 {%0,%1}, [%2], %3;"
+                     : "=r"(v[0]), "=r"(v[1]) : "l"(p), "l"(pol));
+    } else {
+        v[0] = ld_stream(p, pol);
+    }
 }
 
 // L lanes per row, R rows per lane group per step.  Within a step every load that
@@ -400,6 +472,188 @@ __global__ void __launch_bounds__(1024) k_iter(IterArgs<VT, GT> a, int it) {
     if (MODE == M_CHECK) {
         block_sum_to(acc_r, &a.ctrl->acc[PRIMAL ? A_RX2 : A_RY2]);
         block_sum_to(acc_d, &a.ctrl->acc[PRIMAL ? A_DXA2 : A_DYA2]);
+    }
+}
+
+// The same iteration over the SELL-32 copy: one warp per slice, one lane per row,
+// so there are no row pointers to load and no shuffles, every lane of a slice runs
+// the same number of chunks, and each chunk is one vector load of W values and one
+// of W indices per lane (the warp reads 32 W contiguous elements of each).  Two
+// chunks are loaded before either is consumed.  The row's own vectors are read
+// with the slice offsets, coalesced (internal numbering).  Each CTA owns a
+// contiguous range of slices.  Sums and updates are FP64.
+template <typename VT, typename GT, int W, int MODE, bool PRIMAL>
+__global__ void __launch_bounds__(1024) k_iter_sell(IterArgs<VT, GT> a, int it) {
+    const Ctrl* ctrl = a.ctrl;
+    if (ctrl->done) return;
+    const unsigned long long pol = evict_first_policy();
+    const double kk = (double)(ctrl->k_base + it);
+    const double wk = (kk + 1.0) / (kk + 2.0);
+    const double wa = 1.0 / (kk + 2.0);
+    const double step = PRIMAL ? ctrl->tau : ctrl->sigma;
+    const double rho = a.rho;
+    const int lane = threadIdx.x & 31;
+    const int wpc = blockDim.x >> 5;
+    const int nsl = (a.rows + 31) >> 5;
+    const int per_cta = (nsl + (int)gridDim.x - 1) / (int)gridDim.x;
+    const int s0 = min(nsl, (int)blockIdx.x * per_cta);
+    const int s1 = min(nsl, s0 + per_cta);
+    double acc_r = 0.0, acc_d = 0.0;
+    for (int sl = s0 + (threadIdx.x >> 5); sl < s1; sl += wpc) {
+        const int row = sl * 32 + lane;
+        const bool valid = row < a.rows;
+        const long long p0 = ld_stream((const long long*)a.soff + sl, pol);
+        const long long p1 = ld_stream((const long long*)a.soff + sl + 1, pol);
+        const double zr = valid ? a.z[row] : 0.0;
+        const double cst = valid ? a.cost[row] : 0.0;
+        const double zan = valid ? a.za[row] : 0.0;
+        double lo, hi = 0.0;
+        if (PRIMAL) {
+            lo = valid ? a.lo[row] : 0.0;
+            hi = valid ? a.hi[row] : 0.0;
+        } else {
+            lo = (valid && !a.is_eq[row]) ? (a.ylb ? a.ylb[row] : 0.0) : -INFINITY;
+        }
+        const int nq = (int)((p1 - p0) / (32 * W));
+        const VT* vp = a.val + p0 + lane * W;
+        const int* ip = a.idx + p0 + lane * W;
+        double s_0 = 0.0, s_1 = 0.0;
+        int q = 0;
+        for (; q + 2 <= nq; q += 2) {
+            VT v0[W], v1[W];
+            int c0[W], c1[W];
+            ld_stream_w<W>(vp + (int64_t)q * 32 * W, v0, pol);
+            ld_stream_w<W>(ip + (int64_t)q * 32 * W, c0, pol);
+            ld_stream_w<W>(vp + (int64_t)(q + 1) * 32 * W, v1, pol);
+            ld_stream_w<W>(ip + (int64_t)(q + 1) * 32 * W, c1, pol);
+            GT g0[W], g1[W];
+#pragma unroll
+            for (int e = 0; e < W; ++e) {
+                g0[e] = a.gather[c0[e]];
+                g1[e] = a.gather[c1[e]];
+            }
+#pragma unroll
+            for (int e = 0; e < W; ++e) {
+                s_0 += (double)v0[e] * (double)g0[e];
+                s_1 += (double)v1[e] * (double)g1[e];
+            }
+        }
+        if (q < nq) {
+            VT v0[W];
+            int c0[W];
+            ld_stream_w<W>(vp + (int64_t)q * 32 * W, v0, pol);
+            ld_stream_w<W>(ip + (int64_t)q * 32 * W, c0, pol);
+#pragma unroll
+            for (int e = 0; e < W; ++e) s_0 += (double)v0[e] * (double)a.gather[c0[e]];
+        }
+        if (!valid) continue;
+        const double s = s_0 + s_1;
+        double zt;
+        if (PRIMAL) {
+            zt = clampT(zr - step * (cst + s), lo, hi);
+            a.zh[row] = (VT)(2.0 * zt - zr);
+        } else {
+            zt = zr + step * (s - cst);
+            if (zt < lo) zt = lo;  // -inf on equality rows; NaN stays NaN
+        }
+        a.z[row] = wk * ((1.0 + rho) * zt - rho * zr) + wa * zan;
+        if (MODE != M_PLAIN) {
+            const double d = zr - zt;
+            acc_r += d * d;
+        }
+        if (MODE == M_CHECK) {
+            a.zt[row] = zt;
+            const double e = zt - zan;
+            acc_d += e * e;
+        }
+    }
+    if (MODE == M_FIRST) block_sum_to(acc_r, &a.ctrl->acc[PRIMAL ? A_RX2_FIRST : A_RY2_FIRST]);
+    if (MODE == M_CHECK) {
+        block_sum_to(acc_r, &a.ctrl->acc[PRIMAL ? A_RX2 : A_RY2]);
+        block_sum_to(acc_d, &a.ctrl->acc[PRIMAL ? A_DXA2 : A_DYA2]);
+    }
+}
+
+// ------------------------------------------------------------------ internal numbering and SELL copies (setup)
+// key of row i: (window, decreasing length) -> a stable radix sort orders each window by length
+__global__ void k_len_keys(int rows, const int32_t* __restrict__ ptr, int wlog, unsigned long long* __restrict__ keys,
+                           int32_t* __restrict__ ids) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < rows; i += gridDim.x * blockDim.x) {
+        const unsigned len = (unsigned)(ptr[i + 1] - ptr[i]);
+        keys[i] = ((unsigned long long)(i >> wlog) << 32) | (unsigned long long)(0xFFFFFFFFu - len);
+        ids[i] = i;
+    }
+}
+
+__global__ void k_invert(int rows, const int32_t* __restrict__ perm, int32_t* __restrict__ inv) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < rows; i += gridDim.x * blockDim.x) inv[perm[i]] = i;
+}
+
+// out[i + 1] = length of original row perm[i] (out[0] = 0; scanned afterwards)
+__global__ void k_perm_lens(int rows, const int32_t* __restrict__ perm, const int32_t* __restrict__ ptr,
+                            int32_t* __restrict__ out) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < rows; i += gridDim.x * blockDim.x) {
+        const int r = perm[i];
+        out[i + 1] = ptr[r + 1] - ptr[r];
+        if (i == 0) out[0] = 0;
+    }
+}
+
+// internal row i = original row perm[i], its indices renumbered by imap
+__global__ void k_perm_csr(int rows, const int32_t* __restrict__ perm, const int32_t* __restrict__ ptr,
+                           const int32_t* __restrict__ idx, const double* __restrict__ val,
+                           const int32_t* __restrict__ imap, const int32_t* __restrict__ optr,
+                           int32_t* __restrict__ oidx, double* __restrict__ oval) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < rows; i += gridDim.x * blockDim.x) {
+        const int r = perm[i];
+        const int k0 = ptr[r], len = ptr[r + 1] - k0, o = optr[i];
+        for (int e = 0; e < len; ++e) {
+            oidx[o + e] = imap[idx[k0 + e]];
+            oval[o + e] = val[k0 + e];
+        }
+    }
+}
+
+template <typename T>
+__global__ void k_gather_perm(int rows, const int32_t* __restrict__ perm, const T* __restrict__ src, T* __restrict__ dst) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < rows; i += gridDim.x * blockDim.x) dst[i] = src[perm[i]];
+}
+
+template <typename T>
+__global__ void k_scatter_perm(int rows, const int32_t* __restrict__ perm, const T* __restrict__ src, T* __restrict__ dst) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < rows; i += gridDim.x * blockDim.x) dst[perm[i]] = src[i];
+}
+
+// longest row of every 32-row slice
+__global__ void k_slice_len(int rows, const int32_t* __restrict__ ptr, int32_t* __restrict__ slen) {
+    const int nsl = (rows + 31) >> 5;
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < nsl; s += gridDim.x * blockDim.x) {
+        int mx = 0;
+        for (int r = s * 32; r < min(rows, s * 32 + 32); ++r) mx = max(mx, ptr[r + 1] - ptr[r]);
+        slen[s] = mx;
+    }
+}
+
+// SELL position of entry e of row i
+__device__ __forceinline__ int64_t sell_pos(const int64_t* off, int W, int i, int e) {
+    return off[i >> 5] + (int64_t)(e / W) * 32 * W + (i & 31) * W + (e % W);
+}
+
+// indices of the SELL copy (padding stays as zero-filled)
+__global__ void k_sell_idx(int rows, const int32_t* __restrict__ ptr, const int32_t* __restrict__ idx,
+                           const int64_t* __restrict__ off, int W, int32_t* __restrict__ sidx) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < rows; i += gridDim.x * blockDim.x) {
+        const int k0 = ptr[i], len = ptr[i + 1] - k0;
+        for (int e = 0; e < len; ++e) sidx[sell_pos(off, W, i, e)] = idx[k0 + e];
+    }
+}
+
+template <typename VT>
+__global__ void k_sell_vals(int rows, const int32_t* __restrict__ ptr, const double* __restrict__ v64,
+                            const int64_t* __restrict__ off, int W, VT* __restrict__ sval) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < rows; i += gridDim.x * blockDim.x) {
+        const int k0 = ptr[i], len = ptr[i + 1] - k0;
+        for (int e = 0; e < len; ++e) sval[sell_pos(off, W, i, e)] = (VT)v64[k0 + e];
     }
 }
 
@@ -662,7 +916,7 @@ void launch_kkt(int Lr, int Lc, unsigned gr, unsigned gc, cudaStream_t s, const 
 
 // Scaling, scaled copies and ||A_s||_2 (FP64, once per uploaded LP and ruiz count).
 int prepare_scaling(Ctx* ctx, HalpernWork* w, int ruiz_iters, bool need32) {
-    DevLP& L = ctx->lp;
+    DevLP& L = w->ilp;
     cudaStream_t s = ctx->stream;
     const int m = L.m, n = L.n;
     unsigned gm = grid_for(m, TB, ctx->sm_count), gn = grid_for(n, TB, ctx->sm_count);
@@ -693,7 +947,7 @@ int prepare_scaling(Ctx* ctx, HalpernWork* w, int ruiz_iters, bool need32) {
 
 // sigma_max(A_s)^2 by power iteration on A_s^T A_s; rounds of 16 until the estimate settles.
 int power_sigma2(Ctx* ctx, HalpernWork* w, double* sigma2) {
-    DevLP& L = ctx->lp;
+    DevLP& L = w->ilp;
     cudaStream_t s = ctx->stream;
     const int m = L.m, n = L.n;
     unsigned gm = grid_for(m, TB, ctx->sm_count), gn = grid_for(n, TB, ctx->sm_count, 4);
@@ -732,6 +986,156 @@ int power_sigma2(Ctx* ctx, HalpernWork* w, double* sigma2) {
     return B2P_OK;
 }
 
+// Rows (or columns) sorted by decreasing length inside windows of 2^kWindowLog
+// (stable: equal lengths keep their order).  perm: internal -> original, inv: the inverse.
+constexpr int kWindowLog = 12;
+
+int sort_by_length(Ctx* ctx, int rows, const int32_t* ptr, int32_t* perm, int32_t* inv) {
+    cudaStream_t s = ctx->stream;
+    DBuf<unsigned long long> keys, keys_out;
+    DBuf<int32_t> ids;
+    B2P_CUDA(ctx, keys.reserve(rows));
+    B2P_CUDA(ctx, keys_out.reserve(rows));
+    B2P_CUDA(ctx, ids.reserve(rows));
+    const unsigned g = grid_for(rows, TB, ctx->sm_count);
+    k_len_keys<<<g, TB, 0, s>>>(rows, ptr, kWindowLog, keys.p, ids.p);
+    B2P_LAUNCH(ctx);
+    int end_bit = 33;
+    while (end_bit < 64 && (1LL << (end_bit - 32)) <= ((rows - 1) >> kWindowLog)) ++end_bit;
+    size_t tmp = 0;
+    B2P_CUDA(ctx, cub::DeviceRadixSort::SortPairs(nullptr, tmp, keys.p, keys_out.p, ids.p, perm, rows, 0, end_bit, s));
+    B2P_CUDA(ctx, ctx->cub_tmp.reserve(tmp));
+    tmp = ctx->cub_tmp.bytes();
+    B2P_CUDA(ctx, cub::DeviceRadixSort::SortPairs(ctx->cub_tmp.p, tmp, keys.p, keys_out.p, ids.p, perm, rows, 0, end_bit, s));
+    k_invert<<<g, TB, 0, s>>>(rows, perm, inv);
+    B2P_LAUNCH(ctx);
+    ctx->launches += 2;
+    B2P_CUDA(ctx, cudaStreamSynchronize(s));  // temporaries are freed on return
+    return B2P_OK;
+}
+
+// One orientation of the internal CSR: internal row i is original row perm[i], its
+// indices renumbered through imap.
+int permute_csr(Ctx* ctx, int rows, const int32_t* perm, const int32_t* ptr, const int32_t* idx, const double* val,
+                const int32_t* imap, int32_t* optr, int32_t* oidx, double* oval) {
+    cudaStream_t s = ctx->stream;
+    const unsigned g = grid_for(rows, TB, ctx->sm_count);
+    k_perm_lens<<<g, TB, 0, s>>>(rows, perm, ptr, optr);
+    B2P_LAUNCH(ctx);
+    size_t tmp = 0;
+    B2P_CUDA(ctx, cub::DeviceScan::InclusiveSum(nullptr, tmp, optr + 1, optr + 1, rows, s));
+    B2P_CUDA(ctx, ctx->cub_tmp.reserve(tmp));
+    tmp = ctx->cub_tmp.bytes();
+    B2P_CUDA(ctx, cub::DeviceScan::InclusiveSum(ctx->cub_tmp.p, tmp, optr + 1, optr + 1, rows, s));
+    k_perm_csr<<<g, TB, 0, s>>>(rows, perm, ptr, idx, val, imap, optr, oidx, oval);
+    B2P_LAUNCH(ctx);
+    ctx->launches += 2;
+    return B2P_OK;
+}
+
+// The uploaded LP in internal numbering (once per upload).
+int build_internal(Ctx* ctx, HalpernWork* w) {
+    const DevLP& U = ctx->lp;
+    DevLP& I = w->ilp;
+    cudaStream_t s = ctx->stream;
+    const int m = U.m, n = U.n;
+    const int64_t nnz = U.nnz;
+    I.m = m;
+    I.n = n;
+    I.nnz = nnz;
+    for (auto* b : {&w->pr, &w->ir}) B2P_CUDA(ctx, b->reserve(m));
+    for (auto* b : {&w->pc, &w->ic}) B2P_CUDA(ctx, b->reserve(n));
+    B2P_CUDA(ctx, I.rowptr.reserve(m + 1));
+    B2P_CUDA(ctx, I.t_rowptr.reserve(n + 1));
+    for (auto* b : {&I.colidx, &I.t_colidx}) B2P_CUDA(ctx, b->reserve(nnz));
+    for (auto* b : {&I.vals, &I.t_vals}) B2P_CUDA(ctx, b->reserve(nnz));
+    B2P_CUDA(ctx, I.b.reserve(m));
+    B2P_CUDA(ctx, I.is_eq.reserve(m));
+    for (auto* b : {&I.c, &I.lb, &I.ub}) B2P_CUDA(ctx, b->reserve(n));
+    int st = sort_by_length(ctx, m, U.rowptr.p, w->pr.p, w->ir.p);
+    if (st) return st;
+    st = sort_by_length(ctx, n, U.t_rowptr.p, w->pc.p, w->ic.p);
+    if (st) return st;
+    st = permute_csr(ctx, m, w->pr.p, U.rowptr.p, U.colidx.p, U.vals.p, w->ic.p, I.rowptr.p, I.colidx.p, I.vals.p);
+    if (st) return st;
+    st = permute_csr(ctx, n, w->pc.p, U.t_rowptr.p, U.t_colidx.p, U.t_vals.p, w->ir.p, I.t_rowptr.p, I.t_colidx.p,
+                     I.t_vals.p);
+    if (st) return st;
+    const unsigned gm = grid_for(m, TB, ctx->sm_count), gn = grid_for(n, TB, ctx->sm_count);
+    k_gather_perm<double><<<gm, TB, 0, s>>>(m, w->pr.p, U.b.p, I.b.p);
+    k_gather_perm<uint8_t><<<gm, TB, 0, s>>>(m, w->pr.p, U.is_eq.p, I.is_eq.p);
+    k_gather_perm<double><<<gn, TB, 0, s>>>(n, w->pc.p, U.c.p, I.c.p);
+    k_gather_perm<double><<<gn, TB, 0, s>>>(n, w->pc.p, U.lb.p, I.lb.p);
+    k_gather_perm<double><<<gn, TB, 0, s>>>(n, w->pc.p, U.ub.p, I.ub.p);
+    B2P_LAUNCH(ctx);
+    ctx->launches += 5;
+    I.bnorm = U.bnorm;
+    I.cnorm = U.cnorm;
+    I.mean_row_len = U.mean_row_len;
+    I.mean_col_len = U.mean_col_len;
+    I.max_row_len = U.max_row_len;
+    I.max_col_len = U.max_col_len;
+    w->sr.idx_ready = w->sc.idx_ready = false;
+    B2P_CUDA(ctx, cudaStreamSynchronize(s));
+    w->ilp_gen = ctx->lp_gen;
+    return B2P_OK;
+}
+
+// Slice layout and indices of a SELL copy (once per upload): vector width W = 4 or 2
+// when its padding costs at most 3 % over W = 1 (which pads only to each slice's
+// longest row).
+int build_sell_layout(Ctx* ctx, Sell& S, int rows, const int32_t* ptr, const int32_t* idx) {
+    cudaStream_t s = ctx->stream;
+    const int nsl = (rows + 31) / 32;
+    DBuf<int32_t> slen;
+    B2P_CUDA(ctx, slen.reserve(nsl));
+    k_slice_len<<<grid_for(nsl, TB, ctx->sm_count), TB, 0, s>>>(rows, ptr, slen.p);
+    B2P_LAUNCH(ctx);
+    std::vector<int32_t> h(nsl);
+    B2P_CUDA(ctx, cudaMemcpyAsync(h.data(), slen.p, sizeof(int32_t) * nsl, cudaMemcpyDeviceToHost, s));
+    B2P_CUDA(ctx, cudaStreamSynchronize(s));
+    auto padded_total = [&](int W) {
+        int64_t t = 0;
+        for (int v : h) t += 32LL * ((v + W - 1) / W * W);
+        return t;
+    };
+    const int64_t t1 = padded_total(1);
+    int W = 1;
+    if (padded_total(4) <= t1 + t1 * 3 / 100) W = 4;
+    else if (padded_total(2) <= t1 + t1 * 3 / 100) W = 2;
+    std::vector<int64_t> off(nsl + 1, 0);
+    for (int i = 0; i < nsl; ++i) off[i + 1] = off[i] + 32LL * ((h[i] + W - 1) / W * W);
+    S.W = W;
+    S.slices = nsl;
+    S.total = off[nsl];
+    B2P_CUDA(ctx, S.off.reserve(nsl + 1));
+    B2P_CUDA(ctx, S.idx.reserve(std::max<int64_t>(S.total, 1)));
+    B2P_CUDA(ctx, cudaMemcpyAsync(S.off.p, off.data(), sizeof(int64_t) * (nsl + 1), cudaMemcpyHostToDevice, s));
+    B2P_CUDA(ctx, cudaMemsetAsync(S.idx.p, 0, sizeof(int32_t) * std::max<int64_t>(S.total, 1), s));
+    k_sell_idx<<<grid_for(rows, TB, ctx->sm_count), TB, 0, s>>>(rows, ptr, idx, S.off.p, W, S.idx.p);
+    B2P_LAUNCH(ctx);
+    ctx->launches += 2;
+    B2P_CUDA(ctx, cudaStreamSynchronize(s));  // slen is freed on return, h / off are host temporaries
+    S.idx_ready = true;
+    // the value copies belong to the old layout
+    S.v32.release();
+    S.v64.release();
+    return B2P_OK;
+}
+
+// Scaled values into a SELL copy (every solve: the scaling depends on the Ruiz count).
+template <typename VT>
+int fill_sell_vals(Ctx* ctx, Sell& S, int rows, const int32_t* ptr, const double* v64, DBuf<VT>& out) {
+    cudaStream_t s = ctx->stream;
+    const bool fresh = out.p == nullptr;
+    B2P_CUDA(ctx, out.reserve(std::max<int64_t>(S.total, 1)));
+    if (fresh) B2P_CUDA(ctx, cudaMemsetAsync(out.p, 0, sizeof(VT) * std::max<int64_t>(S.total, 1), s));
+    k_sell_vals<VT><<<grid_for(rows, TB, ctx->sm_count), TB, 0, s>>>(rows, ptr, v64, S.off.p, S.W, out.p);
+    B2P_LAUNCH(ctx);
+    ctx->launches += 1;
+    return B2P_OK;
+}
+
 template <typename MT>
 struct Ops;
 template <>
@@ -739,26 +1143,60 @@ struct Ops<double> {
     static const double* sv(HalpernWork* w) { return w->sv64.p; }
     static const double* stv(HalpernWork* w) { return w->stv64.p; }
     static double* xh(HalpernWork* w) { return w->xh64.p; }
+    static DBuf<double>& sell(Sell& S) { return S.v64; }
 };
 template <>
 struct Ops<float> {
     static const float* sv(HalpernWork* w) { return w->sv32.p; }
     static const float* stv(HalpernWork* w) { return w->stv32.p; }
     static float* xh(HalpernWork* w) { return w->xh32.p; }
+    static DBuf<float>& sell(Sell& S) { return S.v32; }
 };
 
-// Arguments of the primal kernel (A^T y over the CSR of A^T, updates x) and of the
-// dual kernel (A xh over the CSR of A, updates y; with re-centring its sign bound
-// on <= rows is the shifted ylb_s).
+// Arguments of the primal kernel (A^T y over A^T, updates x) and of the dual kernel
+// (A xh over A, updates y; with re-centring its sign bound on <= rows is the shifted
+// ylb_s), over the CSR copies or (sell = true) the SELL copies.
 template <typename MT>
-IterArgs<MT, double> primal_args(const DevLP& L, HalpernWork* w, const b2p_params* p) {
-    return {L.t_rowptr.p, L.t_colidx.p, Ops<MT>::stv(w), w->y.p, w->c64.p, w->l64.p, w->u64.p, nullptr, nullptr,
-            w->x.p, Ops<MT>::xh(w), w->xa.p, w->xt.p, w->ctrl.p, L.n, p->reflection};
+IterArgs<MT, double> primal_args(const DevLP& L, HalpernWork* w, const b2p_params* p, bool sell) {
+    IterArgs<MT, double> a{L.t_rowptr.p, L.t_colidx.p, Ops<MT>::stv(w), w->y.p, w->c64.p, w->l64.p, w->u64.p,
+                           nullptr, nullptr, w->x.p, Ops<MT>::xh(w), w->xa.p, w->xt.p, w->ctrl.p, L.n,
+                           p->reflection, nullptr};
+    if (sell) {
+        a.ptr = nullptr;
+        a.idx = w->sc.idx.p;
+        a.val = Ops<MT>::sell(w->sc).p;
+        a.soff = w->sc.off.p;
+    }
+    return a;
 }
 template <typename MT>
-IterArgs<MT, MT> dual_args(const DevLP& L, HalpernWork* w, const b2p_params* p) {
-    return {L.rowptr.p, L.colidx.p, Ops<MT>::sv(w), Ops<MT>::xh(w), w->b64.p, nullptr, nullptr, L.is_eq.p,
-            w->recenter ? w->ylb_s.p : nullptr, w->y.p, nullptr, w->ya.p, w->yt.p, w->ctrl.p, L.m, p->reflection};
+IterArgs<MT, MT> dual_args(const DevLP& L, HalpernWork* w, const b2p_params* p, bool sell) {
+    IterArgs<MT, MT> a{L.rowptr.p, L.colidx.p, Ops<MT>::sv(w), Ops<MT>::xh(w), w->b64.p, nullptr, nullptr, L.is_eq.p,
+                       w->recenter ? w->ylb_s.p : nullptr, w->y.p, nullptr, w->ya.p, w->yt.p, w->ctrl.p, L.m,
+                       p->reflection, nullptr};
+    if (sell) {
+        a.ptr = nullptr;
+        a.idx = w->sr.idx.p;
+        a.val = Ops<MT>::sell(w->sr).p;
+        a.soff = w->sr.off.p;
+    }
+    return a;
+}
+
+template <typename VT, typename GT, int MODE, bool PRIMAL>
+void launch_sell_W(int W, unsigned grid, int tb, cudaStream_t s, const IterArgs<VT, GT>& a, int it) {
+    switch (W) {
+        case 4: k_iter_sell<VT, GT, 4, MODE, PRIMAL><<<grid, tb, 0, s>>>(a, it); break;
+        case 2: k_iter_sell<VT, GT, 2, MODE, PRIMAL><<<grid, tb, 0, s>>>(a, it); break;
+        default: k_iter_sell<VT, GT, 1, MODE, PRIMAL><<<grid, tb, 0, s>>>(a, it); break;
+    }
+}
+
+template <typename VT, typename GT, bool PRIMAL>
+void launch_sell(int mode, int W, unsigned grid, int tb, cudaStream_t s, const IterArgs<VT, GT>& a, int it) {
+    if (mode == M_FIRST) launch_sell_W<VT, GT, M_FIRST, PRIMAL>(W, grid, tb, s, a, it);
+    else if (mode == M_CHECK) launch_sell_W<VT, GT, M_CHECK, PRIMAL>(W, grid, tb, s, a, it);
+    else launch_sell_W<VT, GT, M_PLAIN, PRIMAL>(W, grid, tb, s, a, it);
 }
 
 // One resident wave: 2048 / tb CTAs per SM, each owning a contiguous row range.
@@ -766,16 +1204,20 @@ inline unsigned iter_grid(int64_t rows, int L, int R, int tb, int sm_count) {
     return grid_for((rows * L + R - 1) / R, tb, sm_count, 2048 / tb);
 }
 
-// Times candidate (L, R, CTA size) launch shapes of the primal and dual kernels
-// on the uploaded LP (plain iterations from the current iterates, CUDA events on
-// the context stream) and keeps the fastest of each.  The caller re-initialises
-// the iterates afterwards.  Explicit lanes_per_row skips the search.
+// Times candidate launch shapes of the primal and dual kernels on the uploaded LP
+// (plain iterations from the current iterates, CUDA events on the context stream)
+// and keeps the fastest of each side: the SELL kernel with CTA sizes 256 / 512 /
+// 1024, and the CSR kernel with (L lanes per row, R rows per lane group, CTA size).
+// The caller re-initialises the iterates afterwards.  lanes_per_row > 0 forces the
+// CSR kernel with that L, -1 the SELL kernel (CTA size 256); both skip the search.
 template <typename MT>
 int autotune_shapes(Ctx* ctx, HalpernWork* w, const b2p_params* p) {
-    DevLP& L = ctx->lp;
+    DevLP& L = w->ilp;
     const long long key = ((long long)L.nnz * 1000003LL + (long long)L.m * 101LL + L.n) * 2 + (sizeof(MT) == 4);
-    if (p->lanes_per_row > 0) {
-        w->Lc = w->Lr = pick_lanes(0, p->lanes_per_row);
+    if (p->lanes_per_row != 0) {
+        const bool sell = p->lanes_per_row < 0;
+        w->sell_c = w->sell_r = sell;
+        w->Lc = w->Lr = sell ? 1 : pick_lanes(0, p->lanes_per_row);
         w->Rc = w->Rr = 1;
         w->Tc = w->Tr = 256;
         w->tuned_key = -1;
@@ -784,46 +1226,59 @@ int autotune_shapes(Ctx* ctx, HalpernWork* w, const b2p_params* p) {
     if (w->tuned_key == key) return B2P_OK;
     cudaStream_t s = ctx->stream;
     const int m = L.m, n = L.n;
-    Ctrl* ctrl = w->ctrl.p;
-    const IterArgs<MT, double> pa = primal_args<MT>(L, w, p);
-    const IterArgs<MT, MT> da = dual_args<MT>(L, w, p);
+    const IterArgs<MT, double> pa = primal_args<MT>(L, w, p, false), pas = primal_args<MT>(L, w, p, true);
+    const IterArgs<MT, MT> da = dual_args<MT>(L, w, p, false), das = dual_args<MT>(L, w, p, true);
     cudaEvent_t e0, e1;
     B2P_CUDA(ctx, cudaEventCreate(&e0));
     B2P_CUDA(ctx, cudaEventCreate(&e1));
     for (int side = 0; side < 2; ++side) {
         const bool primal = side == 0;
+        const int64_t rows = primal ? n : m;
         const double mean = primal ? L.mean_col_len : L.mean_row_len;
         const int base_L = pick_lanes(mean, 0);
         float best = 1e30f;
         int bestL = base_L, bestR = 1, bestT = 256;
+        bool bestS = false;
+        auto trial = [&](bool sell, int Lc, int R, int tb) -> int {
+            const unsigned g = sell ? iter_grid(rows, 1, 1, tb, ctx->sm_count) : iter_grid(rows, Lc, R, tb, ctx->sm_count);
+            float tot = 0.f;
+            for (int rep = 0; rep < 4; ++rep) {
+                cudaEventRecord(e0, s);
+                if (sell && primal) launch_sell<MT, double, true>(M_PLAIN, w->sc.W, g, tb, s, pas, rep);
+                else if (sell) launch_sell<MT, MT, false>(M_PLAIN, w->sr.W, g, tb, s, das, rep);
+                else if (primal) launch_iter<MT, double, true>(M_PLAIN, Lc, R, g, tb, s, pa, rep);
+                else launch_iter<MT, MT, false>(M_PLAIN, Lc, R, g, tb, s, da, rep);
+                cudaEventRecord(e1, s);
+                B2P_LAUNCH(ctx);
+                B2P_CUDA(ctx, cudaEventSynchronize(e1));
+                float ms = 0.f;
+                cudaEventElapsedTime(&ms, e0, e1);
+                if (rep > 0) tot += ms;  // first launch warms caches
+            }
+            ctx->launches += 4;
+            if (tot < best) {
+                best = tot;
+                bestS = sell;
+                bestL = Lc;
+                bestR = R;
+                bestT = tb;
+            }
+            return B2P_OK;
+        };
+        for (int tb : {256, 512, 1024}) {
+            int st = trial(true, 1, 1, tb);
+            if (st) return st;
+        }
         for (int Lc : {base_L / 2, base_L, base_L * 2}) {
             if (Lc < 2 || Lc > 32) continue;
-            for (int R : {1, 2, 4}) for (int tb : {256, 512, 1024}) {
-                const int64_t rows = primal ? n : m;
-                unsigned g = iter_grid(rows, Lc, R, tb, ctx->sm_count);
-                float tot = 0.f;
-                for (int rep = 0; rep < 4; ++rep) {
-                    cudaEventRecord(e0, s);
-                    if (primal) launch_iter<MT, double, true>(M_PLAIN, Lc, R, g, tb, s, pa, rep);
-                    else launch_iter<MT, MT, false>(M_PLAIN, Lc, R, g, tb, s, da, rep);
-                    cudaEventRecord(e1, s);
-                    B2P_LAUNCH(ctx);
-                    B2P_CUDA(ctx, cudaEventSynchronize(e1));
-                    float ms = 0.f;
-                    cudaEventElapsedTime(&ms, e0, e1);
-                    if (rep > 0) tot += ms;  // first launch warms caches
+            for (int R : {1, 2, 4})
+                for (int tb : {256, 512, 1024}) {
+                    int st = trial(false, Lc, R, tb);
+                    if (st) return st;
                 }
-                ctx->launches += 4;
-                if (tot < best) {
-                    best = tot;
-                    bestL = Lc;
-                    bestR = R;
-                    bestT = tb;
-                }
-            }
         }
-        if (primal) { w->Lc = bestL; w->Rc = bestR; w->Tc = bestT; }
-        else { w->Lr = bestL; w->Rr = bestR; w->Tr = bestT; }
+        if (primal) { w->sell_c = bestS; w->Lc = bestL; w->Rc = bestR; w->Tc = bestT; }
+        else { w->sell_r = bestS; w->Lr = bestL; w->Rr = bestR; w->Tr = bestT; }
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
@@ -833,31 +1288,31 @@ int autotune_shapes(Ctx* ctx, HalpernWork* w, const b2p_params* p) {
 
 template <typename MT>
 int run_chunks(Ctx* ctx, HalpernWork* w, const b2p_params* p, double time_limit_ms, double t_start) {
-    DevLP& L = ctx->lp;
+    DevLP& L = w->ilp;
     cudaStream_t s = ctx->stream;
     const int m = L.m, n = L.n, K = p->check_every;
     const int Lr = w->Lr, Lc = w->Lc, Rr = w->Rr, Rc = w->Rc, Tr = w->Tr, Tc = w->Tc;
     // R = 1 grids serve the two reduction iterations; the KKT kernels use 256-thread grids
     unsigned gr = iter_grid(m, Lr, 1, Tr, ctx->sm_count), gc = iter_grid(n, Lc, 1, Tc, ctx->sm_count);
     unsigned grR = iter_grid(m, Lr, Rr, Tr, ctx->sm_count), gcR = iter_grid(n, Lc, Rc, Tc, ctx->sm_count);
-    unsigned gkr = iter_grid(m, Lr, 1, TB, ctx->sm_count), gkc = iter_grid(n, Lc, 1, TB, ctx->sm_count);
+    const int Lkr = pick_lanes(L.mean_row_len, 0), Lkc = pick_lanes(L.mean_col_len, 0);
+    unsigned gkr = iter_grid(m, Lkr, 1, TB, ctx->sm_count), gkc = iter_grid(n, Lkc, 1, TB, ctx->sm_count);
     Ctrl* ctrl = w->ctrl.p;
-    const IterArgs<MT, double> pa = primal_args<MT>(L, w, p);
-    const IterArgs<MT, MT> da = dual_args<MT>(L, w, p);
+    const IterArgs<MT, double> pa = primal_args<MT>(L, w, p, w->sell_c);
+    const IterArgs<MT, MT> da = dual_args<MT>(L, w, p, w->sell_r);
     auto chunk = [&]() {
         for (int i = 0; i < K; ++i) {
             int mode = (i == 0) ? M_FIRST : (i == K - 1 ? M_CHECK : M_PLAIN);
-            if (mode == M_PLAIN) {
-                launch_iter<MT, double, true>(mode, Lc, Rc, gcR, Tc, s, pa, i);
-                launch_iter<MT, MT, false>(mode, Lr, Rr, grR, Tr, s, da, i);
-            } else {
-                launch_iter<MT, double, true>(mode, Lc, 1, gc, Tc, s, pa, i);
-                launch_iter<MT, MT, false>(mode, Lr, 1, gr, Tr, s, da, i);
-            }
+            if (w->sell_c) launch_sell<MT, double, true>(mode, w->sc.W, gc, Tc, s, pa, i);
+            else if (mode == M_PLAIN) launch_iter<MT, double, true>(mode, Lc, Rc, gcR, Tc, s, pa, i);
+            else launch_iter<MT, double, true>(mode, Lc, 1, gc, Tc, s, pa, i);
+            if (w->sell_r) launch_sell<MT, MT, false>(mode, w->sr.W, gr, Tr, s, da, i);
+            else if (mode == M_PLAIN) launch_iter<MT, MT, false>(mode, Lr, Rr, grR, Tr, s, da, i);
+            else launch_iter<MT, MT, false>(mode, Lr, 1, gr, Tr, s, da, i);
         }
         const KktMap map = w->recenter ? KktMap{w->xbar.p, w->ybar.p, w->axbar.p, w->atybar.p}
                                        : KktMap{nullptr, nullptr, nullptr, nullptr};
-        launch_kkt(Lr, Lc, gkr, gkc, s, L, w, map, ctrl);
+        launch_kkt(Lkr, Lkc, gkr, gkc, s, L, w, map, ctrl);
         k_control<<<1, 1, 0, s>>>(ctrl);
         const unsigned gv = grid_for(std::max(m, n), TB, ctx->sm_count, 8);
         if (w->recenter) {
@@ -929,7 +1384,7 @@ int run_chunks(Ctx* ctx, HalpernWork* w, const b2p_params* p, double time_limit_
 template <typename MT>
 int solve_T(Ctx* ctx, HalpernWork* w, const b2p_params* p, const double* x0, const double* y0, b2p_result* r,
             double* x_out, double* y_out) {
-    DevLP& L = ctx->lp;
+    DevLP& L = w->ilp;
     cudaStream_t s = ctx->stream;
     const int m = L.m, n = L.n;
     const bool mixed = sizeof(MT) == 4;
@@ -956,6 +1411,18 @@ int solve_T(Ctx* ctx, HalpernWork* w, const b2p_params* p, const double* x0, con
     }
     int st = prepare_scaling(ctx, w, p->ruiz_iterations, mixed);
     if (st) return st;
+    if (!w->sr.idx_ready) {
+        st = build_sell_layout(ctx, w->sr, m, L.rowptr.p, L.colidx.p);
+        if (st) return st;
+    }
+    if (!w->sc.idx_ready) {
+        st = build_sell_layout(ctx, w->sc, n, L.t_rowptr.p, L.t_colidx.p);
+        if (st) return st;
+    }
+    st = fill_sell_vals<MT>(ctx, w->sr, m, L.rowptr.p, w->sv64.p, Ops<MT>::sell(w->sr));
+    if (st) return st;
+    st = fill_sell_vals<MT>(ctx, w->sc, n, L.t_rowptr.p, w->stv64.p, Ops<MT>::sell(w->sc));
+    if (st) return st;
     double sig2 = 0.0;
     st = power_sigma2(ctx, w, &sig2);
     if (st) return st;
@@ -977,13 +1444,19 @@ int solve_T(Ctx* ctx, HalpernWork* w, const b2p_params* p, const double* x0, con
     // warm start (original space) -> device temporaries
     const double* x0d = nullptr;
     const double* y0d = nullptr;
-    if (x0) {
+    if (x0) {  // original -> internal numbering (pv / pu are free after the power iteration)
         B2P_CUDA(ctx, cudaMemcpyAsync(w->tmp_n.p, x0, sizeof(double) * n, cudaMemcpyHostToDevice, s));
-        x0d = w->tmp_n.p;
+        k_gather_perm<double><<<grid_for(n, TB, ctx->sm_count), TB, 0, s>>>(n, w->pc.p, w->tmp_n.p, w->pv.p);
+        B2P_LAUNCH(ctx);
+        ctx->launches += 1;
+        x0d = w->pv.p;
     }
     if (y0) {
         B2P_CUDA(ctx, cudaMemcpyAsync(w->tmp_m.p, y0, sizeof(double) * m, cudaMemcpyHostToDevice, s));
-        y0d = w->tmp_m.p;
+        k_gather_perm<double><<<grid_for(m, TB, ctx->sm_count), TB, 0, s>>>(m, w->pr.p, w->tmp_m.p, w->pu.p);
+        B2P_LAUNCH(ctx);
+        ctx->launches += 1;
+        y0d = w->pu.p;
     }
     k_init_iterates<<<grid_for(std::max(m, n), TB, ctx->sm_count), TB, 0, s>>>(
         m, n, w->l64.p, w->u64.p, x0d, y0d, w->dr.p, w->dc.p, L.is_eq.p, nullptr, w->x.p, w->xa.p, w->xt.p, w->y.p, w->ya.p,
@@ -1024,6 +1497,8 @@ int solve_T(Ctx* ctx, HalpernWork* w, const b2p_params* p, const double* x0, con
             B2P_CUDA(ctx, cudaMemcpyAsync(w->ctrl.p, &hc, sizeof(Ctrl), cudaMemcpyHostToDevice, s));
         }
     }
+    w->solved_gen = ctx->lp_gen;
+    w->solved_precision = p->precision;
     B2P_CUDA(ctx, cudaEventRecord(ctx->ev0, s));
     st = run_chunks<MT>(ctx, w, p, p->time_limit_s * 1000.0, t_start);
     B2P_CUDA(ctx, cudaEventRecord(ctx->ev1, s));
@@ -1051,10 +1526,13 @@ int solve_T(Ctx* ctx, HalpernWork* w, const b2p_params* p, const double* x0, con
         k_unscale<<<grid_for(std::max(m, n), TB, ctx->sm_count), TB, 0, s>>>(
             m, n, w->xt.p, w->yt.p, w->dr.p, w->dc.p, w->recenter ? w->xbar.p : nullptr,
             w->recenter ? w->ybar.p : nullptr, w->tmp_n.p, w->tmp_m.p);
+        // internal -> original numbering
+        k_scatter_perm<double><<<grid_for(n, TB, ctx->sm_count), TB, 0, s>>>(n, w->pc.p, w->tmp_n.p, w->pv.p);
+        k_scatter_perm<double><<<grid_for(m, TB, ctx->sm_count), TB, 0, s>>>(m, w->pr.p, w->tmp_m.p, w->pu.p);
         B2P_LAUNCH(ctx);
-        ctx->launches += 1;
-        if (x_out) B2P_CUDA(ctx, cudaMemcpyAsync(x_out, w->tmp_n.p, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
-        if (y_out) B2P_CUDA(ctx, cudaMemcpyAsync(y_out, w->tmp_m.p, sizeof(double) * m, cudaMemcpyDeviceToHost, s));
+        ctx->launches += 3;
+        if (x_out) B2P_CUDA(ctx, cudaMemcpyAsync(x_out, w->pv.p, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
+        if (y_out) B2P_CUDA(ctx, cudaMemcpyAsync(y_out, w->pu.p, sizeof(double) * m, cudaMemcpyDeviceToHost, s));
         B2P_CUDA(ctx, cudaStreamSynchronize(s));
         r->transfer_time_ms += now_ms() - t0;
     }
@@ -1064,11 +1542,12 @@ int solve_T(Ctx* ctx, HalpernWork* w, const b2p_params* p, const double* x0, con
 template <typename MT>
 int kernel_timing_T(Ctx* ctx, HalpernWork* w, const b2p_params* p, int reps, double* pms, double* dms, double* pb,
                     double* db) {
-    DevLP& L = ctx->lp;
+    DevLP& L = w->ilp;
     cudaStream_t s = ctx->stream;
     const int m = L.m, n = L.n;
     const int Lr = w->Lr, Lc = w->Lc, Rr = w->Rr, Rc = w->Rc, Tr = w->Tr, Tc = w->Tc;
-    unsigned gr = iter_grid(m, Lr, Rr, Tr, ctx->sm_count), gc = iter_grid(n, Lc, Rc, Tc, ctx->sm_count);
+    unsigned gr = iter_grid(m, Lr, w->sell_r ? 1 : Rr, Tr, ctx->sm_count);
+    unsigned gc = iter_grid(n, Lc, w->sell_c ? 1 : Rc, Tc, ctx->sm_count);
     Ctrl* ctrl = w->ctrl.p;
     // re-open the (finished) control block for plain iterations, restore it afterwards
     Ctrl saved;
@@ -1077,16 +1556,18 @@ int kernel_timing_T(Ctx* ctx, HalpernWork* w, const b2p_params* p, int reps, dou
     Ctrl open = saved;
     open.done = 0;
     B2P_CUDA(ctx, cudaMemcpyAsync(ctrl, &open, sizeof(Ctrl), cudaMemcpyHostToDevice, s));
-    const IterArgs<MT, double> pa = primal_args<MT>(L, w, p);
-    const IterArgs<MT, MT> da = dual_args<MT>(L, w, p);
+    const IterArgs<MT, double> pa = primal_args<MT>(L, w, p, w->sell_c);
+    const IterArgs<MT, MT> da = dual_args<MT>(L, w, p, w->sell_r);
     cudaEvent_t e[3];
     for (auto& x : e) B2P_CUDA(ctx, cudaEventCreate(&x));
     double tp = 0, td = 0;
     for (int r = 0; r < reps; ++r) {
         cudaEventRecord(e[0], s);
-        launch_iter<MT, double, true>(M_PLAIN, Lc, Rc, gc, Tc, s, pa, r);
+        if (w->sell_c) launch_sell<MT, double, true>(M_PLAIN, w->sc.W, gc, Tc, s, pa, r);
+        else launch_iter<MT, double, true>(M_PLAIN, Lc, Rc, gc, Tc, s, pa, r);
         cudaEventRecord(e[1], s);
-        launch_iter<MT, MT, false>(M_PLAIN, Lr, Rr, gr, Tr, s, da, r);
+        if (w->sell_r) launch_sell<MT, MT, false>(M_PLAIN, w->sr.W, gr, Tr, s, da, r);
+        else launch_iter<MT, MT, false>(M_PLAIN, Lr, Rr, gr, Tr, s, da, r);
         cudaEventRecord(e[2], s);
         B2P_LAUNCH(ctx);
         B2P_CUDA(ctx, cudaEventSynchronize(e[2]));
@@ -1102,12 +1583,15 @@ int kernel_timing_T(Ctx* ctx, HalpernWork* w, const b2p_params* p, int reps, dou
     B2P_CUDA(ctx, cudaStreamSynchronize(s));
     *pms = tp / reps;
     *dms = td / reps;
-    // algorithmic bytes: every matrix entry, row pointer and vector element once
+    // algorithmic bytes: every matrix entry, row pointer (CSR) or slice offset (SELL) and
+    // vector element once; SELL padding is not counted
     const double vb = sizeof(MT), nnz = (double)L.nnz;
+    const double pc_bytes = w->sell_c ? 8.0 * (w->sc.slices + 1) : 4.0 * (n + 1);
+    const double pr_bytes = w->sell_r ? 8.0 * (w->sr.slices + 1) : 4.0 * (m + 1);
     // primal: A^T values+indices, col pointers, gather y (m x 8), x r/w, xa, c, l, u (8 each), xh write
-    *pb = nnz * (vb + 4) + 4.0 * (n + 1) + 8.0 * m + n * (8 * 6 + vb);
+    *pb = nnz * (vb + 4) + pc_bytes + 8.0 * m + n * (8 * 6 + vb);
     // dual: A values+indices, row pointers, gather xh (n x vb), y r/w, ya, b (8 each), is_eq (1)
-    *db = nnz * (vb + 4) + 4.0 * (m + 1) + vb * n + m * (8 * 4 + 1);
+    *db = nnz * (vb + 4) + pr_bytes + vb * n + m * (8 * 4 + 1);
     return B2P_OK;
 }
 
@@ -1116,6 +1600,10 @@ int kernel_timing_T(Ctx* ctx, HalpernWork* w, const b2p_params* p, int reps, dou
 int halpern_kernel_timing(Ctx* ctx, const b2p_params* p, int reps, double* primal_ms, double* dual_ms,
                           double* primal_bytes, double* dual_bytes) {
     HalpernWork* w = ctx->hw;
+    if (w->solved_gen != ctx->lp_gen || w->solved_precision != p->precision) {
+        ctx->err = "b2p_kernel_timing: the last solve of the uploaded LP used another precision (or none ran)";
+        return B2P_NO_LP;
+    }
     if (p->precision == B2P_FP32) {
         if (!w->xh32.p || !w->sv32.p) {
             ctx->err = "b2p_kernel_timing: no mixed-precision solve to time";
@@ -1140,9 +1628,13 @@ int halpern_engine_solve(Ctx* ctx, const b2p_params* p, const double* x0, const 
         ctx->err = "unknown precision";
         return B2P_INVALID_ARGUMENT;
     }
-    DevLP& L = ctx->lp;
     if (!ctx->hw) ctx->hw = new HalpernWork();
     HalpernWork* w = ctx->hw;
+    if (w->ilp_gen != ctx->lp_gen) {
+        int st = build_internal(ctx, w);
+        if (st) return st;
+    }
+    DevLP& L = w->ilp;
     const int m = L.m, n = L.n;
     const int64_t nnz = L.nnz;
     w->m = m;

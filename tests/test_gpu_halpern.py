@@ -142,3 +142,49 @@ def test_mixed_without_refinement_matches_fp64_iterations_at_1e6(ctx, lps):
     r32, _, _ = ctx.solve(engine="halpern", precision="fp32", eps=1e-6)
     assert r64["status"] == r32["status"] == "OPTIMAL"
     assert abs(r64["iterations"] - r32["iterations"]) <= 2 * 64
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+@pytest.mark.parametrize("kernel", ["sell", "csr"])
+@pytest.mark.parametrize("name", ["rs_c0", "ba_tiny", "ill_small"])
+def test_iteration_kernel_variants(ctx, golden, lps, name, precision, kernel):
+    """Both iteration kernels -- SELL-32 over the length-sorted internal numbering
+    (lanes_per_row = -1) and sub-warp CSR (lanes_per_row = 8) -- reach the tolerance,
+    and the answer, mapped back to the caller's numbering, matches the oracle's KKT
+    and the HiGHS optimum."""
+    std = lps[name].standard()
+    ctx.upload(std)
+    eps = 1e-8 if name == "ill_small" else 1e-6
+    res, x, y = ctx.solve(engine="halpern", precision=precision, eps=eps, max_iterations=400000,
+                          lanes_per_row=-1 if kernel == "sell" else 8)
+    assert res["status"] == "OPTIMAL", res
+    k = pdlp_oracle.kkt(std, x, y)
+    assert k["rel_kkt"] <= 1.05 * eps, k
+    z = golden["highs"][name]
+    tol = 1e-5 if (name == "ill_small" and precision == "fp32") else 1e-6
+    assert abs(k["pobj"] - z) <= tol * max(1.0, abs(z)), (k["pobj"], z)
+
+
+def test_sell_and_csr_agree_on_iterates(ctx, lps):
+    """The two kernels compute the same iteration up to FP64 summation order: on the
+    block-angular LP (rows and columns renumbered by the SELL layout) a fixed number
+    of FP64 iterations gives the same point to ~1e-9."""
+    std = lps["ba_tiny"].standard()
+    ctx.upload(std)
+    ra, xa, ya = ctx.solve(engine="halpern", precision="fp64", eps=0.0, max_iterations=512, lanes_per_row=-1)
+    rb, xb, yb = ctx.solve(engine="halpern", precision="fp64", eps=0.0, max_iterations=512, lanes_per_row=8)
+    assert ra["iterations"] == rb["iterations"] == 512
+    assert np.allclose(xa, xb, rtol=1e-9, atol=1e-9 * (1 + np.abs(xb).max()))
+    assert np.allclose(ya, yb, rtol=1e-9, atol=1e-9 * (1 + np.abs(yb).max()))
+
+
+def test_warm_start_is_renumbered(ctx, lps):
+    """A warm start in the caller's numbering lands on the right rows and columns of the
+    internal numbering: restarting from the answer of a block-angular LP stops at once."""
+    std = lps["ba_tiny"].standard()
+    ctx.upload(std)
+    res, x, y = ctx.solve(engine="halpern", precision="fp64", eps=1e-8, max_iterations=400000, lanes_per_row=-1)
+    assert res["status"] == "OPTIMAL"
+    res2, x2, y2 = ctx.solve(x0=x, y0=y, engine="halpern", precision="fp64", eps=1e-6, lanes_per_row=-1,
+                             primal_weight=res["primal_weight"])
+    assert res2["status"] == "OPTIMAL" and res2["iterations"] <= 128, res2
