@@ -115,7 +115,9 @@ typedef struct {
                                        FP64 matrix.  -1 = on for FP32 / off for FP64 (default), 0 = off,
                                        > 0 = on */
     double  time_limit_s;           /* 0 = none */
-    int     lanes_per_row;          /* 0 = auto; else 1,2,4,8,16,32 lanes per CSR row */
+    int     lanes_per_row;          /* Halpern engine iteration kernels: 0 = autotuned; 1,2,4,8,16,32 =
+                                       CSR kernel with that many lanes per row; -1 = SELL-32 kernel;
+                                       -2 = SELL-32 kernel with gather windows in shared memory */
 } b2p_params;
 
 typedef struct {

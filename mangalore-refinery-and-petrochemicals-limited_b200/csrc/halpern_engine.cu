@@ -26,10 +26,20 @@
 // captured once as a CUDA graph and replayed until the control block says done.
 //
 // Kernels per iteration (HBM-bound; algorithmic bytes in kernel_timing_T below):
-//   k_primal : A^T y (CSR of A^T, L lanes per column) + projected primal step
-//              + extrapolation + Halpern update (+ check reductions)
-//   k_dual   : A xh  (CSR of A,   L lanes per row)    + projected dual step
-//              + Halpern update (+ check reductions)
+//   primal : A^T y + projected primal step + extrapolation + Halpern update
+//            (+ check reductions)
+//   dual   : A xh  + projected dual step + Halpern update (+ check reductions)
+// each in one of three forms, picked per side by an autotuner on the uploaded LP:
+//   k_iter_sell           SELL-32 copy of the operator (one lane per row, W-wide
+//                         vector loads, no row pointers, no shuffles)
+//   k_iter_sell<...,WIN>  the same, with each CTA's densest window of the gathered
+//                         vector staged in shared memory
+//   k_iter                CSR, L lanes per row, R rows per lane group
+// The engine works on the LP renumbered so that rows and columns are sorted by
+// length inside windows of 4096 (k_len_keys): the 32 rows of a SELL slice then have
+// nearly equal lengths while rows that were neighbours stay near each other.
+// Warm starts and answers are mapped between the caller's and the internal
+// numbering on the device.
 #include <cub/cub.cuh>
 
 #include <cmath>
@@ -80,6 +90,13 @@ struct Sell {
     bool idx_ready = false;
 };
 
+// Per-CTA gather windows for one launch shape of a windowed SELL kernel.
+struct Win {
+    unsigned G = 0;      // grid (one resident wave)
+    size_t smem = 0;     // dynamic shared memory per CTA (bytes); 0 = windows off
+    DBuf<int32_t> lo, len;
+};
+
 struct HalpernWork {
     int m = -1, n = -1;
     // Internal numbering: rows and columns sorted by decreasing length inside
@@ -92,6 +109,9 @@ struct HalpernWork {
     DBuf<int32_t> ic, ir;        // original -> internal column / row
     Sell sr, sc;                 // SELL copies of A (rows) and A^T (columns)
     bool sell_r = false, sell_c = false;  // tuned: SELL (true) or CSR kernel per side
+    // tuned gather windows of the SELL kernels (smem 0 = none): grid, shared memory
+    // bytes and the per-CTA windows built for that grid
+    Win wr, wc;
     int64_t solved_gen = -1;     // upload generation and precision of the last solve
     int solved_precision = -1;   // (the state b2p_kernel_timing replays)
     DBuf<double> dr, dc, tmp_m, tmp_n, pv, pu, pw;
@@ -291,6 +311,8 @@ struct IterArgs {
     int rows;
     double rho;
     const int64_t* soff;   // SELL kernel: slice offsets (ptr / idx / val unused by it except idx, val)
+    const int32_t* win_lo;   // SELL kernel with gather windows: per-CTA window of `gather`
+    const int32_t* win_len;  //   staged in shared memory (len 0 = none)
 };
 
 // Matrix entries and row pointers are read once per iteration: bypass L1 and mark
@@ -482,10 +504,49 @@ __global__ void __launch_bounds__(1024) k_iter(IterArgs<VT, GT> a, int it) {
 // chunks are loaded before either is consumed.  The row's own vectors are read
 // with the slice offsets, coalesced (internal numbering).  Each CTA owns a
 // contiguous range of slices.  Sums and updates are FP64.
-template <typename VT, typename GT, int W, int MODE, bool PRIMAL>
+// WIN: the CTA first copies its window of the gathered vector (k_win_setup) into
+// shared memory and serves the gathers that fall inside it from there -- a random
+// 32-lane gather costs a few shared-memory bank cycles instead of 32 L1 requests.
+template <typename VT, typename GT, int W, int MODE, bool PRIMAL, bool WIN>
 __global__ void __launch_bounds__(1024) k_iter_sell(IterArgs<VT, GT> a, int it) {
     const Ctrl* ctrl = a.ctrl;
     if (ctrl->done) return;
+    extern __shared__ __align__(16) unsigned char win_raw[];
+    GT* gwin = reinterpret_cast<GT*>(win_raw);
+    int wlo = 0;
+    unsigned wlen = 0;
+    if (WIN) {
+        wlo = a.win_lo[blockIdx.x];
+        wlen = (unsigned)a.win_len[blockIdx.x];
+        // 16-byte copies, 8 in flight per thread (the window starts 16-byte aligned:
+        // wlo is a multiple of 4 elements), then the scalar tail
+        constexpr unsigned per16 = 16 / sizeof(GT);
+        const unsigned nvec = wlen / per16;
+        const float4* src = reinterpret_cast<const float4*>(a.gather + wlo);
+        float4* dst = reinterpret_cast<float4*>(gwin);
+        for (unsigned base = threadIdx.x; base < nvec; base += 8 * blockDim.x) {
+            float4 t[8];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {
+                const unsigned j = base + u * blockDim.x;
+                if (j < nvec) t[u] = src[j];
+            }
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {
+                const unsigned j = base + u * blockDim.x;
+                if (j < nvec) dst[j] = t[u];
+            }
+        }
+        for (unsigned j = nvec * per16 + threadIdx.x; j < wlen; j += blockDim.x) gwin[j] = a.gather[wlo + j];
+        __syncthreads();
+    }
+    auto gat = [&](int c) -> GT {
+        if (WIN) {
+            const unsigned o = (unsigned)(c - wlo);
+            return o < wlen ? gwin[o] : a.gather[c];
+        }
+        return a.gather[c];
+    };
     const unsigned long long pol = evict_first_policy();
     const double kk = (double)(ctrl->k_base + it);
     const double wk = (kk + 1.0) / (kk + 2.0);
@@ -529,8 +590,8 @@ __global__ void __launch_bounds__(1024) k_iter_sell(IterArgs<VT, GT> a, int it) 
             GT g0[W], g1[W];
 #pragma unroll
             for (int e = 0; e < W; ++e) {
-                g0[e] = a.gather[c0[e]];
-                g1[e] = a.gather[c1[e]];
+                g0[e] = gat(c0[e]);
+                g1[e] = gat(c1[e]);
             }
 #pragma unroll
             for (int e = 0; e < W; ++e) {
@@ -544,7 +605,7 @@ __global__ void __launch_bounds__(1024) k_iter_sell(IterArgs<VT, GT> a, int it) 
             ld_stream_w<W>(vp + (int64_t)q * 32 * W, v0, pol);
             ld_stream_w<W>(ip + (int64_t)q * 32 * W, c0, pol);
 #pragma unroll
-            for (int e = 0; e < W; ++e) s_0 += (double)v0[e] * (double)a.gather[c0[e]];
+            for (int e = 0; e < W; ++e) s_0 += (double)v0[e] * (double)gat(c0[e]);
         }
         if (!valid) continue;
         const double s = s_0 + s_1;
@@ -639,12 +700,56 @@ __device__ __forceinline__ int64_t sell_pos(const int64_t* off, int W, int i, in
     return off[i >> 5] + (int64_t)(e / W) * 32 * W + (i & 31) * W + (e % W);
 }
 
-// indices of the SELL copy (padding stays as zero-filled)
+// indices of the SELL copy; a padding slot repeats an index of its own row (or of the
+// slice's first, longest row), so padding stays inside the row's neighbourhood of the
+// gathered vector (its value is 0)
 __global__ void k_sell_idx(int rows, const int32_t* __restrict__ ptr, const int32_t* __restrict__ idx,
                            const int64_t* __restrict__ off, int W, int32_t* __restrict__ sidx) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < rows; i += gridDim.x * blockDim.x) {
         const int k0 = ptr[i], len = ptr[i + 1] - k0;
+        const int s = i >> 5;
+        const int plen = (int)((off[s + 1] - off[s]) >> 5);
         for (int e = 0; e < len; ++e) sidx[sell_pos(off, W, i, e)] = idx[k0 + e];
+        if (plen > len) {
+            const int first = ptr[s * 32];
+            const int pad = len > 0 ? idx[k0 + len - 1] : (ptr[s * 32 + 1] > first ? idx[first] : 0);
+            for (int e = len; e < plen; ++e) sidx[sell_pos(off, W, i, e)] = pad;
+        }
+    }
+}
+
+// Gather windows: CTA b of a grid of G over `rows` rows (contiguous ranges of
+// per_cta slices, as the iteration kernel assigns them) stages the part
+// [lo_b, lo_b + len_b) of the gathered vector in shared memory.  The window is
+// the pair of adjacent buckets (bucket = cap / 2 elements) holding most of the
+// CTA's entries; len_b = 0 (no staging) when it holds less than half of them.
+__global__ void k_win_setup(int rows, const int32_t* __restrict__ ptr, const int32_t* __restrict__ idx,
+                            int per_cta, int n_other, int cap, int nb, int32_t* __restrict__ wlo,
+                            int32_t* __restrict__ wlen) {
+    extern __shared__ int hist[];
+    const int nsl = (rows + 31) >> 5;
+    const int b = blockIdx.x;
+    const int s0 = min(nsl, b * per_cta), s1 = min(nsl, s0 + per_cta);
+    const int r0 = min(rows, s0 * 32), r1 = min(rows, s1 * 32);
+    const int bucket = cap / 2;
+    for (int j = threadIdx.x; j < nb; j += blockDim.x) hist[j] = 0;
+    __syncthreads();
+    const int e0 = ptr[r0], e1 = ptr[r1];
+    for (int e = e0 + threadIdx.x; e < e1; e += blockDim.x) atomicAdd(&hist[idx[e] / bucket], 1);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int best = -1, bj = 0;
+        for (int j = 0; j < nb; ++j) {
+            const int c = hist[j] + (j + 1 < nb ? hist[j + 1] : 0);
+            if (c > best) { best = c; bj = j; }
+        }
+        const int total = e1 - e0;
+        int lo = bj * bucket, len = min(cap, n_other - lo);
+        lo &= ~3;  // 16-byte aligned start for either element size
+        len = min(cap, n_other - lo);
+        const bool use = total > 0 && 2 * best >= total;
+        wlo[b] = use ? lo : 0;
+        wlen[b] = use ? len : 0;
     }
 }
 
@@ -1082,8 +1187,8 @@ int build_internal(Ctx* ctx, HalpernWork* w) {
 }
 
 // Slice layout and indices of a SELL copy (once per upload): vector width W = 4 or 2
-// when its padding costs at most 3 % over W = 1 (which pads only to each slice's
-// longest row).
+// when its padding costs at most 3 % over W = 1, which pads only to each slice's
+// longest row.
 int build_sell_layout(Ctx* ctx, Sell& S, int rows, const int32_t* ptr, const int32_t* idx) {
     cudaStream_t s = ctx->stream;
     const int nsl = (rows + 31) / 32;
@@ -1099,10 +1204,11 @@ int build_sell_layout(Ctx* ctx, Sell& S, int rows, const int32_t* ptr, const int
         for (int v : h) t += 32LL * ((v + W - 1) / W * W);
         return t;
     };
+    const int pad_pct = 3;  // padding allowed for the wider vectors, percent of the W = 1 layout
     const int64_t t1 = padded_total(1);
     int W = 1;
-    if (padded_total(4) <= t1 + t1 * 3 / 100) W = 4;
-    else if (padded_total(2) <= t1 + t1 * 3 / 100) W = 2;
+    if (padded_total(4) <= t1 + t1 * pad_pct / 100) W = 4;
+    else if (padded_total(2) <= t1 + t1 * pad_pct / 100) W = 2;
     std::vector<int64_t> off(nsl + 1, 0);
     for (int i = 0; i < nsl; ++i) off[i + 1] = off[i] + 32LL * ((h[i] + W - 1) / W * W);
     S.W = W;
@@ -1136,6 +1242,36 @@ int fill_sell_vals(Ctx* ctx, Sell& S, int rows, const int32_t* ptr, const double
     return B2P_OK;
 }
 
+// Gather windows of one orientation for a windowed launch of `tb` threads and `smem`
+// bytes of shared memory per CTA over a one-wave grid (per_sm CTAs per SM); gsize =
+// bytes per gathered element.  Leaves W.smem = 0 when the gathered vector is too long for the bucket
+// histogram (more than 16384 buckets).
+int build_windows(Ctx* ctx, Win& W, int rows, const int32_t* ptr, const int32_t* idx, int n_other, int tb,
+                  size_t smem, size_t gsize, int per_sm) {
+    cudaStream_t s = ctx->stream;
+    W.smem = 0;
+    // one resident wave of `per_sm` CTAs per SM (the kernel's occupancy at this shape)
+    if (per_sm < 1) return B2P_OK;
+    const unsigned G = (unsigned)(ctx->sm_count * per_sm);
+    const int nsl = (rows + 31) / 32;
+    const int per_cta = (nsl + (int)G - 1) / (int)G;
+    const int cap = (int)(smem / gsize);
+    const int bucket = cap / 2;
+    const long long nb = ((long long)n_other + bucket - 1) / bucket;
+    if (bucket < 1 || nb > 16384) return B2P_OK;
+    B2P_CUDA(ctx, W.lo.reserve(G));
+    B2P_CUDA(ctx, W.len.reserve(G));
+    const size_t hbytes = sizeof(int) * (size_t)nb;
+    if (hbytes > 48 * 1024)
+        B2P_CUDA(ctx, cudaFuncSetAttribute(k_win_setup, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hbytes));
+    k_win_setup<<<G, 256, hbytes, s>>>(rows, ptr, idx, per_cta, n_other, cap, (int)nb, W.lo.p, W.len.p);
+    B2P_LAUNCH(ctx);
+    ctx->launches += 1;
+    W.G = G;
+    W.smem = smem;
+    return B2P_OK;
+}
+
 template <typename MT>
 struct Ops;
 template <>
@@ -1166,6 +1302,8 @@ IterArgs<MT, double> primal_args(const DevLP& L, HalpernWork* w, const b2p_param
         a.idx = w->sc.idx.p;
         a.val = Ops<MT>::sell(w->sc).p;
         a.soff = w->sc.off.p;
+        a.win_lo = w->wc.lo.p;
+        a.win_len = w->wc.len.p;
     }
     return a;
 }
@@ -1179,24 +1317,53 @@ IterArgs<MT, MT> dual_args(const DevLP& L, HalpernWork* w, const b2p_params* p, 
         a.idx = w->sr.idx.p;
         a.val = Ops<MT>::sell(w->sr).p;
         a.soff = w->sr.off.p;
+        a.win_lo = w->wr.lo.p;
+        a.win_len = w->wr.len.p;
     }
     return a;
 }
 
-template <typename VT, typename GT, int MODE, bool PRIMAL>
-void launch_sell_W(int W, unsigned grid, int tb, cudaStream_t s, const IterArgs<VT, GT>& a, int it) {
+// Largest dynamic shared memory any windowed SELL launch asks for (bytes); every
+// windowed instantiation is opened up to it once per process.
+constexpr int kWinSmemMax = 200 * 1024;
+
+template <typename VT, typename GT, int W, int MODE, bool PRIMAL, bool WIN>
+void launch_sell_one(unsigned grid, int tb, size_t smem, cudaStream_t s, const IterArgs<VT, GT>& a, int it) {
+    if (WIN) {
+        static unsigned long long opened = 0;  // host-side, per instantiation: one bit per device
+        int dev = 0;
+        cudaGetDevice(&dev);
+        if (dev < 64 && !((opened >> dev) & 1ull)) {
+            cudaFuncSetAttribute(k_iter_sell<VT, GT, W, MODE, PRIMAL, WIN>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, kWinSmemMax);
+            opened |= 1ull << dev;
+        }
+    }
+    k_iter_sell<VT, GT, W, MODE, PRIMAL, WIN><<<grid, tb, WIN ? smem : 0, s>>>(a, it);
+}
+
+template <typename VT, typename GT, int MODE, bool PRIMAL, bool WIN>
+void launch_sell_W(int W, unsigned grid, int tb, size_t smem, cudaStream_t s, const IterArgs<VT, GT>& a, int it) {
     switch (W) {
-        case 4: k_iter_sell<VT, GT, 4, MODE, PRIMAL><<<grid, tb, 0, s>>>(a, it); break;
-        case 2: k_iter_sell<VT, GT, 2, MODE, PRIMAL><<<grid, tb, 0, s>>>(a, it); break;
-        default: k_iter_sell<VT, GT, 1, MODE, PRIMAL><<<grid, tb, 0, s>>>(a, it); break;
+        case 4: launch_sell_one<VT, GT, 4, MODE, PRIMAL, WIN>(grid, tb, smem, s, a, it); break;
+        case 2: launch_sell_one<VT, GT, 2, MODE, PRIMAL, WIN>(grid, tb, smem, s, a, it); break;
+        default: launch_sell_one<VT, GT, 1, MODE, PRIMAL, WIN>(grid, tb, smem, s, a, it); break;
     }
 }
 
+// smem > 0: windowed variant (a.win_lo / a.win_len set for this grid), else plain SELL
 template <typename VT, typename GT, bool PRIMAL>
-void launch_sell(int mode, int W, unsigned grid, int tb, cudaStream_t s, const IterArgs<VT, GT>& a, int it) {
-    if (mode == M_FIRST) launch_sell_W<VT, GT, M_FIRST, PRIMAL>(W, grid, tb, s, a, it);
-    else if (mode == M_CHECK) launch_sell_W<VT, GT, M_CHECK, PRIMAL>(W, grid, tb, s, a, it);
-    else launch_sell_W<VT, GT, M_PLAIN, PRIMAL>(W, grid, tb, s, a, it);
+void launch_sell(int mode, int W, unsigned grid, int tb, size_t smem, cudaStream_t s, const IterArgs<VT, GT>& a,
+                 int it) {
+    if (smem > 0) {
+        if (mode == M_FIRST) launch_sell_W<VT, GT, M_FIRST, PRIMAL, true>(W, grid, tb, smem, s, a, it);
+        else if (mode == M_CHECK) launch_sell_W<VT, GT, M_CHECK, PRIMAL, true>(W, grid, tb, smem, s, a, it);
+        else launch_sell_W<VT, GT, M_PLAIN, PRIMAL, true>(W, grid, tb, smem, s, a, it);
+    } else {
+        if (mode == M_FIRST) launch_sell_W<VT, GT, M_FIRST, PRIMAL, false>(W, grid, tb, 0, s, a, it);
+        else if (mode == M_CHECK) launch_sell_W<VT, GT, M_CHECK, PRIMAL, false>(W, grid, tb, 0, s, a, it);
+        else launch_sell_W<VT, GT, M_PLAIN, PRIMAL, false>(W, grid, tb, 0, s, a, it);
+    }
 }
 
 // One resident wave: 2048 / tb CTAs per SM, each owning a contiguous row range.
@@ -1204,12 +1371,44 @@ inline unsigned iter_grid(int64_t rows, int L, int R, int tb, int sm_count) {
     return grid_for((rows * L + R - 1) / R, tb, sm_count, 2048 / tb);
 }
 
+// Shapes of the windowed SELL kernel tried by the tuner: (CTA size, shared memory bytes).
+constexpr int kWinShapes[3][2] = {{1024, 192 * 1024}, {512, 96 * 1024}, {256, 48 * 1024}};
+
+// Resident CTAs per SM of the windowed SELL kernel for one launch shape.
+template <typename VT, typename GT, bool PRIMAL>
+int sell_win_per_sm(int W, int tb, size_t smem) {
+    int per = 0;
+    auto q = [&](auto kern) {
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, kWinSmemMax);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, tb, smem);
+    };
+    if (W == 4) q(k_iter_sell<VT, GT, 4, M_PLAIN, PRIMAL, true>);
+    else if (W == 2) q(k_iter_sell<VT, GT, 2, M_PLAIN, PRIMAL, true>);
+    else q(k_iter_sell<VT, GT, 1, M_PLAIN, PRIMAL, true>);
+    return per;
+}
+
+// Windows of one side for shape `k` of kWinShapes (primal gathers y: FP64; dual gathers xh: MT).
+template <typename MT>
+int side_windows(Ctx* ctx, HalpernWork* w, bool primal, int k) {
+    const DevLP& L = w->ilp;
+    const int tb = kWinShapes[k][0];
+    const size_t smem = kWinShapes[k][1];
+    if (primal)
+        return build_windows(ctx, w->wc, L.n, L.t_rowptr.p, L.t_colidx.p, L.m, tb, smem, sizeof(double),
+                             sell_win_per_sm<MT, double, true>(w->sc.W, tb, smem));
+    return build_windows(ctx, w->wr, L.m, L.rowptr.p, L.colidx.p, L.n, tb, smem, sizeof(MT),
+                         sell_win_per_sm<MT, MT, false>(w->sr.W, tb, smem));
+}
+
 // Times candidate launch shapes of the primal and dual kernels on the uploaded LP
 // (plain iterations from the current iterates, CUDA events on the context stream)
 // and keeps the fastest of each side: the SELL kernel with CTA sizes 256 / 512 /
-// 1024, and the CSR kernel with (L lanes per row, R rows per lane group, CTA size).
-// The caller re-initialises the iterates afterwards.  lanes_per_row > 0 forces the
-// CSR kernel with that L, -1 the SELL kernel (CTA size 256); both skip the search.
+// 1024, the SELL kernel with gather windows in shared memory (kWinShapes), and the
+// CSR kernel with (L lanes per row, R rows per lane group, CTA size).  The caller
+// re-initialises the iterates afterwards.  lanes_per_row > 0 forces the CSR kernel
+// with that L, -1 the SELL kernel (CTA size 256), -2 the windowed SELL kernel (CTA
+// size 512, 96 KB); each skips the search.
 template <typename MT>
 int autotune_shapes(Ctx* ctx, HalpernWork* w, const b2p_params* p) {
     DevLP& L = w->ilp;
@@ -1220,14 +1419,20 @@ int autotune_shapes(Ctx* ctx, HalpernWork* w, const b2p_params* p) {
         w->Lc = w->Lr = sell ? 1 : pick_lanes(0, p->lanes_per_row);
         w->Rc = w->Rr = 1;
         w->Tc = w->Tr = 256;
+        w->wc.smem = w->wr.smem = 0;
+        if (p->lanes_per_row == -2) {
+            w->Tc = w->Tr = kWinShapes[1][0];
+            for (int side = 0; side < 2; ++side) {
+                int st = side_windows<MT>(ctx, w, side == 0, 1);
+                if (st) return st;
+            }
+        }
         w->tuned_key = -1;
         return B2P_OK;
     }
     if (w->tuned_key == key) return B2P_OK;
     cudaStream_t s = ctx->stream;
     const int m = L.m, n = L.n;
-    const IterArgs<MT, double> pa = primal_args<MT>(L, w, p, false), pas = primal_args<MT>(L, w, p, true);
-    const IterArgs<MT, MT> da = dual_args<MT>(L, w, p, false), das = dual_args<MT>(L, w, p, true);
     cudaEvent_t e0, e1;
     B2P_CUDA(ctx, cudaEventCreate(&e0));
     B2P_CUDA(ctx, cudaEventCreate(&e1));
@@ -1236,16 +1441,31 @@ int autotune_shapes(Ctx* ctx, HalpernWork* w, const b2p_params* p) {
         const int64_t rows = primal ? n : m;
         const double mean = primal ? L.mean_col_len : L.mean_row_len;
         const int base_L = pick_lanes(mean, 0);
+        Win& win = primal ? w->wc : w->wr;
         float best = 1e30f;
-        int bestL = base_L, bestR = 1, bestT = 256;
+        int bestL = base_L, bestR = 1, bestT = 256, bestWin = -1;
         bool bestS = false;
-        auto trial = [&](bool sell, int Lc, int R, int tb) -> int {
-            const unsigned g = sell ? iter_grid(rows, 1, 1, tb, ctx->sm_count) : iter_grid(rows, Lc, R, tb, ctx->sm_count);
+        // kind 0: CSR (Lc, R, tb); 1: SELL (tb); 2: windowed SELL (shape k)
+        auto trial = [&](int kind, int Lc, int R, int tb, int k) -> int {
+            unsigned g;
+            size_t smem = 0;
+            if (kind == 2) {
+                int st = side_windows<MT>(ctx, w, primal, k);
+                if (st) return st;
+                if (win.smem == 0) return B2P_OK;  // not possible for this LP
+                g = win.G;
+                smem = win.smem;
+            } else {
+                win.smem = 0;
+                g = kind == 1 ? iter_grid(rows, 1, 1, tb, ctx->sm_count) : iter_grid(rows, Lc, R, tb, ctx->sm_count);
+            }
+            const IterArgs<MT, double> pa = primal_args<MT>(L, w, p, kind != 0);
+            const IterArgs<MT, MT> da = dual_args<MT>(L, w, p, kind != 0);
             float tot = 0.f;
             for (int rep = 0; rep < 4; ++rep) {
                 cudaEventRecord(e0, s);
-                if (sell && primal) launch_sell<MT, double, true>(M_PLAIN, w->sc.W, g, tb, s, pas, rep);
-                else if (sell) launch_sell<MT, MT, false>(M_PLAIN, w->sr.W, g, tb, s, das, rep);
+                if (kind != 0 && primal) launch_sell<MT, double, true>(M_PLAIN, w->sc.W, g, tb, smem, s, pa, rep);
+                else if (kind != 0) launch_sell<MT, MT, false>(M_PLAIN, w->sr.W, g, tb, smem, s, da, rep);
                 else if (primal) launch_iter<MT, double, true>(M_PLAIN, Lc, R, g, tb, s, pa, rep);
                 else launch_iter<MT, MT, false>(M_PLAIN, Lc, R, g, tb, s, da, rep);
                 cudaEventRecord(e1, s);
@@ -1258,7 +1478,8 @@ int autotune_shapes(Ctx* ctx, HalpernWork* w, const b2p_params* p) {
             ctx->launches += 4;
             if (tot < best) {
                 best = tot;
-                bestS = sell;
+                bestS = kind != 0;
+                bestWin = kind == 2 ? k : -1;
                 bestL = Lc;
                 bestR = R;
                 bestT = tb;
@@ -1266,16 +1487,25 @@ int autotune_shapes(Ctx* ctx, HalpernWork* w, const b2p_params* p) {
             return B2P_OK;
         };
         for (int tb : {256, 512, 1024}) {
-            int st = trial(true, 1, 1, tb);
+            int st = trial(1, 1, 1, tb, 0);
+            if (st) return st;
+        }
+        for (int k = 0; k < 3; ++k) {
+            int st = trial(2, 1, 1, kWinShapes[k][0], k);
             if (st) return st;
         }
         for (int Lc : {base_L / 2, base_L, base_L * 2}) {
             if (Lc < 2 || Lc > 32) continue;
             for (int R : {1, 2, 4})
                 for (int tb : {256, 512, 1024}) {
-                    int st = trial(false, Lc, R, tb);
+                    int st = trial(0, Lc, R, tb, 0);
                     if (st) return st;
                 }
+        }
+        win.smem = 0;
+        if (bestWin >= 0) {
+            int st = side_windows<MT>(ctx, w, primal, bestWin);
+            if (st) return st;
         }
         if (primal) { w->sell_c = bestS; w->Lc = bestL; w->Rc = bestR; w->Tc = bestT; }
         else { w->sell_r = bestS; w->Lr = bestL; w->Rr = bestR; w->Tr = bestT; }
@@ -1295,6 +1525,8 @@ int run_chunks(Ctx* ctx, HalpernWork* w, const b2p_params* p, double time_limit_
     // R = 1 grids serve the two reduction iterations; the KKT kernels use 256-thread grids
     unsigned gr = iter_grid(m, Lr, 1, Tr, ctx->sm_count), gc = iter_grid(n, Lc, 1, Tc, ctx->sm_count);
     unsigned grR = iter_grid(m, Lr, Rr, Tr, ctx->sm_count), gcR = iter_grid(n, Lc, Rc, Tc, ctx->sm_count);
+    // SELL grids: one thread per row, or the windows' one-wave grid
+    const unsigned grS = w->wr.smem ? w->wr.G : gr, gcS = w->wc.smem ? w->wc.G : gc;
     const int Lkr = pick_lanes(L.mean_row_len, 0), Lkc = pick_lanes(L.mean_col_len, 0);
     unsigned gkr = iter_grid(m, Lkr, 1, TB, ctx->sm_count), gkc = iter_grid(n, Lkc, 1, TB, ctx->sm_count);
     Ctrl* ctrl = w->ctrl.p;
@@ -1303,10 +1535,10 @@ int run_chunks(Ctx* ctx, HalpernWork* w, const b2p_params* p, double time_limit_
     auto chunk = [&]() {
         for (int i = 0; i < K; ++i) {
             int mode = (i == 0) ? M_FIRST : (i == K - 1 ? M_CHECK : M_PLAIN);
-            if (w->sell_c) launch_sell<MT, double, true>(mode, w->sc.W, gc, Tc, s, pa, i);
+            if (w->sell_c) launch_sell<MT, double, true>(mode, w->sc.W, gcS, Tc, w->wc.smem, s, pa, i);
             else if (mode == M_PLAIN) launch_iter<MT, double, true>(mode, Lc, Rc, gcR, Tc, s, pa, i);
             else launch_iter<MT, double, true>(mode, Lc, 1, gc, Tc, s, pa, i);
-            if (w->sell_r) launch_sell<MT, MT, false>(mode, w->sr.W, gr, Tr, s, da, i);
+            if (w->sell_r) launch_sell<MT, MT, false>(mode, w->sr.W, grS, Tr, w->wr.smem, s, da, i);
             else if (mode == M_PLAIN) launch_iter<MT, MT, false>(mode, Lr, Rr, grR, Tr, s, da, i);
             else launch_iter<MT, MT, false>(mode, Lr, 1, gr, Tr, s, da, i);
         }
@@ -1548,6 +1780,8 @@ int kernel_timing_T(Ctx* ctx, HalpernWork* w, const b2p_params* p, int reps, dou
     const int Lr = w->Lr, Lc = w->Lc, Rr = w->Rr, Rc = w->Rc, Tr = w->Tr, Tc = w->Tc;
     unsigned gr = iter_grid(m, Lr, w->sell_r ? 1 : Rr, Tr, ctx->sm_count);
     unsigned gc = iter_grid(n, Lc, w->sell_c ? 1 : Rc, Tc, ctx->sm_count);
+    if (w->sell_r && w->wr.smem) gr = w->wr.G;
+    if (w->sell_c && w->wc.smem) gc = w->wc.G;
     Ctrl* ctrl = w->ctrl.p;
     // re-open the (finished) control block for plain iterations, restore it afterwards
     Ctrl saved;
@@ -1563,10 +1797,10 @@ int kernel_timing_T(Ctx* ctx, HalpernWork* w, const b2p_params* p, int reps, dou
     double tp = 0, td = 0;
     for (int r = 0; r < reps; ++r) {
         cudaEventRecord(e[0], s);
-        if (w->sell_c) launch_sell<MT, double, true>(M_PLAIN, w->sc.W, gc, Tc, s, pa, r);
+        if (w->sell_c) launch_sell<MT, double, true>(M_PLAIN, w->sc.W, gc, Tc, w->wc.smem, s, pa, r);
         else launch_iter<MT, double, true>(M_PLAIN, Lc, Rc, gc, Tc, s, pa, r);
         cudaEventRecord(e[1], s);
-        if (w->sell_r) launch_sell<MT, MT, false>(M_PLAIN, w->sr.W, gr, Tr, s, da, r);
+        if (w->sell_r) launch_sell<MT, MT, false>(M_PLAIN, w->sr.W, gr, Tr, w->wr.smem, s, da, r);
         else launch_iter<MT, MT, false>(M_PLAIN, Lr, Rr, gr, Tr, s, da, r);
         cudaEventRecord(e[2], s);
         B2P_LAUNCH(ctx);

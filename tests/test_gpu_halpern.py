@@ -144,19 +144,22 @@ def test_mixed_without_refinement_matches_fp64_iterations_at_1e6(ctx, lps):
     assert abs(r64["iterations"] - r32["iterations"]) <= 2 * 64
 
 
+KERNELS = {"sell": -1, "sell_window": -2, "csr": 8}
+
+
 @pytest.mark.parametrize("precision", ["fp64", "fp32"])
-@pytest.mark.parametrize("kernel", ["sell", "csr"])
+@pytest.mark.parametrize("kernel", list(KERNELS))
 @pytest.mark.parametrize("name", ["rs_c0", "ba_tiny", "ill_small"])
 def test_iteration_kernel_variants(ctx, golden, lps, name, precision, kernel):
-    """Both iteration kernels -- SELL-32 over the length-sorted internal numbering
-    (lanes_per_row = -1) and sub-warp CSR (lanes_per_row = 8) -- reach the tolerance,
-    and the answer, mapped back to the caller's numbering, matches the oracle's KKT
-    and the HiGHS optimum."""
+    """Every iteration kernel -- SELL-32 over the length-sorted internal numbering
+    (lanes_per_row = -1), the same with per-CTA gather windows in shared memory (-2),
+    and sub-warp CSR (8) -- reaches the tolerance, and the answer, mapped back to the
+    caller's numbering, matches the oracle's KKT and the HiGHS optimum."""
     std = lps[name].standard()
     ctx.upload(std)
     eps = 1e-8 if name == "ill_small" else 1e-6
     res, x, y = ctx.solve(engine="halpern", precision=precision, eps=eps, max_iterations=400000,
-                          lanes_per_row=-1 if kernel == "sell" else 8)
+                          lanes_per_row=KERNELS[kernel])
     assert res["status"] == "OPTIMAL", res
     k = pdlp_oracle.kkt(std, x, y)
     assert k["rel_kkt"] <= 1.05 * eps, k
@@ -171,11 +174,12 @@ def test_sell_and_csr_agree_on_iterates(ctx, lps):
     of FP64 iterations gives the same point to ~1e-9."""
     std = lps["ba_tiny"].standard()
     ctx.upload(std)
-    ra, xa, ya = ctx.solve(engine="halpern", precision="fp64", eps=0.0, max_iterations=512, lanes_per_row=-1)
     rb, xb, yb = ctx.solve(engine="halpern", precision="fp64", eps=0.0, max_iterations=512, lanes_per_row=8)
-    assert ra["iterations"] == rb["iterations"] == 512
-    assert np.allclose(xa, xb, rtol=1e-9, atol=1e-9 * (1 + np.abs(xb).max()))
-    assert np.allclose(ya, yb, rtol=1e-9, atol=1e-9 * (1 + np.abs(yb).max()))
+    for lpr in (-1, -2):
+        ra, xa, ya = ctx.solve(engine="halpern", precision="fp64", eps=0.0, max_iterations=512, lanes_per_row=lpr)
+        assert ra["iterations"] == rb["iterations"] == 512
+        assert np.allclose(xa, xb, rtol=1e-9, atol=1e-9 * (1 + np.abs(xb).max()))
+        assert np.allclose(ya, yb, rtol=1e-9, atol=1e-9 * (1 + np.abs(yb).max()))
 
 
 def test_warm_start_is_renumbered(ctx, lps):
