@@ -66,6 +66,11 @@ def parse():
     ap.add_argument("--eps", type=float, default=None,
                     help="relative KKT tolerance (default 1e-8 for ill_conditioned, else 1e-6)")
     ap.add_argument("--no-fp64", action="store_true", help="skip the plain FP64 comparison leg")
+    ap.add_argument("--time-limit", type=float, default=None,
+                    help="single-LP workloads: seconds per solve before it stops as INTERRUPTED "
+                         "(default 1200 for ill_conditioned, else none)")
+    ap.add_argument("--e2e-steps", type=int, default=None,
+                    help="single-LP workloads: end-to-end steps (default = --steps; 0 skips the e2e leg)")
     ap.add_argument("--cpu-sample-iters", type=int, default=20)
     ap.add_argument("--profile", action="store_true",
                     help="profiling case: one short solve, then the two iteration kernels once each inside the "
@@ -75,6 +80,10 @@ def parse():
         a.steps = 1 if a.workload in ("refinery_learned", "ill_conditioned") else 5
     if a.eps is None:
         a.eps = 1e-8 if a.workload == "ill_conditioned" else 1e-6
+    if a.time_limit is None:
+        a.time_limit = 1200.0 if a.workload == "ill_conditioned" else 0.0
+    if a.e2e_steps is None:
+        a.e2e_steps = a.steps
     return a
 
 
@@ -626,7 +635,7 @@ def main():
     ctx = b2p.Context(local)
     ctx.set_stream(torch.cuda.current_stream().cuda_stream)
     ctx.upload(std)
-    common = dict(engine="halpern", eps=args.eps, max_iterations=2_000_000)
+    common = dict(engine="halpern", eps=args.eps, max_iterations=2_000_000, time_limit_s=args.time_limit)
     # warm-up (also fills the autotune / allocation caches); on the stress LP, whose
     # solve takes minutes, warm-up solves stop after 4096 iterations
     warm = dict(common, max_iterations=4096) if args.workload == "ill_conditioned" else common
@@ -643,7 +652,7 @@ def main():
     clocks = sampler.stop()
     ms_max = max_over_ranks(ms, world)
     solved = sum_over_ranks(float(sum(r["status"] == "OPTIMAL" for r in results)), world)
-    value = (args.steps * world) / (ms_max / 1e3)
+    value = solved / (ms_max / 1e3)  # LPs that reached the tolerance, per second
     launches = int(sum(r["kernel_launches"] for r in results))
     iters = results[-1]["iterations"]
     # plain FP64 PDHG on the same LP and GPU
@@ -653,10 +662,12 @@ def main():
             ctx.solve(precision="fp64", **warm)
         ms64, res64 = timed_solves(ctx, torch, args.steps, world, precision="fp64", **common)
         ms64 = max_over_ranks(ms64, world)
-        fp64 = {"value": (args.steps * world) / (ms64 / 1e3), "unit": "LPs/s", "iterations": res64[-1]["iterations"],
-                "ms_per_step": ms64 / args.steps, "rel_kkt": res64[-1]["rel_kkt"]}
+        solved64 = sum_over_ranks(float(sum(r["status"] == "OPTIMAL" for r in res64)), world)
+        fp64 = {"value": solved64 / (ms64 / 1e3), "unit": "LPs/s", "iterations": res64[-1]["iterations"],
+                "ms_per_step": ms64 / args.steps, "rel_kkt": res64[-1]["rel_kkt"], "solved": int(solved64)}
     # roofline of the dominant kernel (mixed precision), timed live with CUDA events
-    ctx.solve(precision="fp32", **common)
+    # after a (capped) mixed solve has set up the tuned kernels
+    ctx.solve(precision="fp32", **warm)
     kt = ctx.kernel_timing(reps=20, precision="fp32", **common)
     peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
     peak = peaks.get("hbm_gbs", 6650.0)
@@ -693,7 +704,8 @@ def main():
     torch.cuda.synchronize()
     e0.record(stream)
     up_s = solve_s = 0.0
-    for _ in range(args.steps):
+    e2e_status = []
+    for _ in range(args.e2e_steps):
         t0 = time.perf_counter()
         ctx.upload(plp)
         t1 = time.perf_counter()
@@ -701,13 +713,20 @@ def main():
         t2 = time.perf_counter()
         up_s += t1 - t0
         solve_s += t2 - t1
+        e2e_status.append(res["status"])
     e1.record(stream)
     torch.cuda.synchronize()
     barrier(world)
     e2e_ms = max_over_ranks(e0.elapsed_time(e1), world)
-    e2e = {"value": (args.steps * world) / (e2e_ms / 1e3), "unit": "LPs/s", "h2d_bytes_per_step": h2d,
-           "d2h_bytes_per_step": d2h, "upload_ms_per_step": 1e3 * up_s / args.steps,
-           "solve_ms_per_step": 1e3 * solve_s / args.steps, "iterations": res["iterations"]}
+    if args.e2e_steps > 0:
+        e2e_solved = sum_over_ranks(float(sum(r == "OPTIMAL" for r in e2e_status)), world)
+        e2e = {"value": e2e_solved / (e2e_ms / 1e3), "unit": "LPs/s", "h2d_bytes_per_step": h2d,
+               "d2h_bytes_per_step": d2h, "steps": args.e2e_steps,
+               "upload_ms_per_step": 1e3 * up_s / args.e2e_steps, "solve_ms_per_step": 1e3 * solve_s / args.e2e_steps,
+               "iterations": res["iterations"], "solved": int(e2e_solved)}
+    else:
+        e2e = {"value": None, "skipped": "--e2e-steps 0 (each solve of this workload takes minutes)",
+               "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h}
     cpu = None
     if rank == 0 and world == 1:
         cpu = cpu_reference_sample(lp, args.cpu_sample_iters, fp64["iterations"] if fp64 else iters)
@@ -720,8 +739,9 @@ def main():
                                l2=f"inputs larger than L2 (scaled A and A^T: ~{16 * lp.nnz / 1e6:.0f} MB)",
                                engine="halpern/mixed"),
                 "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "gpu_launches": launches,
-                "clocks": clocks, "iterations": iters, "solved": int(solved), "fp64": fp64,
-                "rel_kkt": results[-1]["rel_kkt"]}
+                "clocks": clocks, "iterations": iters, "solved": int(solved), "status": results[-1]["status"],
+                "fp64": fp64, "rel_kkt": results[-1]["rel_kkt"],
+                "time_limit_s": args.time_limit or None}
         print(json.dumps(line), flush=True)
     ctx.close()
     if world > 1:

@@ -116,8 +116,9 @@ typedef struct {
                                        > 0 = on */
     double  time_limit_s;           /* 0 = none */
     int     lanes_per_row;          /* Halpern engine iteration kernels: 0 = autotuned; 1,2,4,8,16,32 =
-                                       CSR kernel with that many lanes per row; -1 = SELL-32 kernel;
-                                       -2 = SELL-32 kernel with gather windows in shared memory */
+                                       CSR kernel with that many lanes per row; -1 = SELL kernel, 32-row
+                                       slices; -2 = the same with gather windows in shared memory;
+                                       -3 / -4 = SELL kernel, 16- / 8-row slices (2 / 4 lanes per row) */
 } b2p_params;
 
 typedef struct {

@@ -81,6 +81,7 @@ constexpr int kInnerDone = 100;
 // load of W consecutive elements per lane reads 32 W contiguous elements.  Rows
 // shorter than the slice's longest are zero-padded (value 0, index 0).
 struct Sell {
+    int C = 32;          // slice height (rows per slice): 32, 16 or 8
     int W = 1;
     int64_t slices = 0, total = 0;
     DBuf<int64_t> off;   // slices + 1
@@ -107,7 +108,11 @@ struct HalpernWork {
     DevLP ilp;
     DBuf<int32_t> pr, pc;        // internal -> original row / column
     DBuf<int32_t> ic, ir;        // original -> internal column / row
-    Sell sr, sc;                 // SELL copies of A (rows) and A^T (columns)
+    // SELL copies of A (rows) and A^T (columns), slice heights 32, 16, 8 (built on demand);
+    // sr / sc point at the tuned one
+    Sell sr_all[3], sc_all[3];
+    Sell* sr = &sr_all[0];
+    Sell* sc = &sc_all[0];
     bool sell_r = false, sell_c = false;  // tuned: SELL (true) or CSR kernel per side
     // tuned gather windows of the SELL kernels (smem 0 = none): grid, shared memory
     // bytes and the per-CTA windows built for that grid
@@ -507,8 +512,14 @@ __global__ void __launch_bounds__(1024) k_iter(IterArgs<VT, GT> a, int it) {
 // WIN: the CTA first copies its window of the gathered vector (k_win_setup) into
 // shared memory and serves the gathers that fall inside it from there -- a random
 // 32-lane gather costs a few shared-memory bank cycles instead of 32 L1 requests.
-template <typename VT, typename GT, int W, int MODE, bool PRIMAL, bool WIN>
+// C < 32: slices of C rows, 32 / C lanes per row; the lanes of a row take every
+// (32 / C)-th chunk, so one warp-wide load still reads 32 W contiguous elements, and
+// their partial sums meet in a shuffle.  Smaller slices give a warp shorter chains
+// and more, finer work units (better balance when there are few slices per warp).
+template <typename VT, typename GT, int W, int C, int MODE, bool PRIMAL, bool WIN>
 __global__ void __launch_bounds__(1024) k_iter_sell(IterArgs<VT, GT> a, int it) {
+    static_assert(C == 32 || C == 16 || C == 8, "slice height");
+    constexpr int LPR = 32 / C;
     const Ctrl* ctrl = a.ctrl;
     if (ctrl->done) return;
     extern __shared__ __align__(16) unsigned char win_raw[];
@@ -554,39 +565,42 @@ __global__ void __launch_bounds__(1024) k_iter_sell(IterArgs<VT, GT> a, int it) 
     const double step = PRIMAL ? ctrl->tau : ctrl->sigma;
     const double rho = a.rho;
     const int lane = threadIdx.x & 31;
+    const int rl = lane % C, sub = lane / C;  // row within the slice, lane group of the row
     const int wpc = blockDim.x >> 5;
-    const int nsl = (a.rows + 31) >> 5;
+    const int nsl = (a.rows + C - 1) / C;
     const int per_cta = (nsl + (int)gridDim.x - 1) / (int)gridDim.x;
     const int s0 = min(nsl, (int)blockIdx.x * per_cta);
     const int s1 = min(nsl, s0 + per_cta);
     double acc_r = 0.0, acc_d = 0.0;
     for (int sl = s0 + (threadIdx.x >> 5); sl < s1; sl += wpc) {
-        const int row = sl * 32 + lane;
+        const int row = sl * C + rl;
         const bool valid = row < a.rows;
+        const bool lead = valid && sub == 0;
         const long long p0 = ld_stream((const long long*)a.soff + sl, pol);
         const long long p1 = ld_stream((const long long*)a.soff + sl + 1, pol);
-        const double zr = valid ? a.z[row] : 0.0;
-        const double cst = valid ? a.cost[row] : 0.0;
-        const double zan = valid ? a.za[row] : 0.0;
+        const double zr = lead ? a.z[row] : 0.0;
+        const double cst = lead ? a.cost[row] : 0.0;
+        const double zan = lead ? a.za[row] : 0.0;
         double lo, hi = 0.0;
         if (PRIMAL) {
-            lo = valid ? a.lo[row] : 0.0;
-            hi = valid ? a.hi[row] : 0.0;
+            lo = lead ? a.lo[row] : 0.0;
+            hi = lead ? a.hi[row] : 0.0;
         } else {
-            lo = (valid && !a.is_eq[row]) ? (a.ylb ? a.ylb[row] : 0.0) : -INFINITY;
+            lo = (lead && !a.is_eq[row]) ? (a.ylb ? a.ylb[row] : 0.0) : -INFINITY;
         }
-        const int nq = (int)((p1 - p0) / (32 * W));
-        const VT* vp = a.val + p0 + lane * W;
-        const int* ip = a.idx + p0 + lane * W;
+        const int nq = (int)((p1 - p0) / (C * W));
+        const VT* vp = a.val + p0 + rl * W;
+        const int* ip = a.idx + p0 + rl * W;
         double s_0 = 0.0, s_1 = 0.0;
-        int q = 0;
-        for (; q + 2 <= nq; q += 2) {
+        // chunk q of this row at vp + q C W; lane group `sub` takes q = sub, sub + LPR, ...
+        int q = sub;
+        for (; q + LPR < nq; q += 2 * LPR) {
             VT v0[W], v1[W];
             int c0[W], c1[W];
-            ld_stream_w<W>(vp + (int64_t)q * 32 * W, v0, pol);
-            ld_stream_w<W>(ip + (int64_t)q * 32 * W, c0, pol);
-            ld_stream_w<W>(vp + (int64_t)(q + 1) * 32 * W, v1, pol);
-            ld_stream_w<W>(ip + (int64_t)(q + 1) * 32 * W, c1, pol);
+            ld_stream_w<W>(vp + (int64_t)q * C * W, v0, pol);
+            ld_stream_w<W>(ip + (int64_t)q * C * W, c0, pol);
+            ld_stream_w<W>(vp + (int64_t)(q + LPR) * C * W, v1, pol);
+            ld_stream_w<W>(ip + (int64_t)(q + LPR) * C * W, c1, pol);
             GT g0[W], g1[W];
 #pragma unroll
             for (int e = 0; e < W; ++e) {
@@ -602,13 +616,15 @@ __global__ void __launch_bounds__(1024) k_iter_sell(IterArgs<VT, GT> a, int it) 
         if (q < nq) {
             VT v0[W];
             int c0[W];
-            ld_stream_w<W>(vp + (int64_t)q * 32 * W, v0, pol);
-            ld_stream_w<W>(ip + (int64_t)q * 32 * W, c0, pol);
+            ld_stream_w<W>(vp + (int64_t)q * C * W, v0, pol);
+            ld_stream_w<W>(ip + (int64_t)q * C * W, c0, pol);
 #pragma unroll
             for (int e = 0; e < W; ++e) s_0 += (double)v0[e] * (double)gat(c0[e]);
         }
-        if (!valid) continue;
-        const double s = s_0 + s_1;
+        double s = s_0 + s_1;
+#pragma unroll
+        for (int o = C; o < 32; o <<= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if (!lead) continue;
         double zt;
         if (PRIMAL) {
             zt = clampT(zr - step * (cst + s), lo, hi);
@@ -685,35 +701,35 @@ __global__ void k_scatter_perm(int rows, const int32_t* __restrict__ perm, const
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < rows; i += gridDim.x * blockDim.x) dst[perm[i]] = src[i];
 }
 
-// longest row of every 32-row slice
-__global__ void k_slice_len(int rows, const int32_t* __restrict__ ptr, int32_t* __restrict__ slen) {
-    const int nsl = (rows + 31) >> 5;
+// longest row of every C-row slice
+__global__ void k_slice_len(int rows, const int32_t* __restrict__ ptr, int C, int32_t* __restrict__ slen) {
+    const int nsl = (rows + C - 1) / C;
     for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < nsl; s += gridDim.x * blockDim.x) {
         int mx = 0;
-        for (int r = s * 32; r < min(rows, s * 32 + 32); ++r) mx = max(mx, ptr[r + 1] - ptr[r]);
+        for (int r = s * C; r < min(rows, s * C + C); ++r) mx = max(mx, ptr[r + 1] - ptr[r]);
         slen[s] = mx;
     }
 }
 
-// SELL position of entry e of row i
-__device__ __forceinline__ int64_t sell_pos(const int64_t* off, int W, int i, int e) {
-    return off[i >> 5] + (int64_t)(e / W) * 32 * W + (i & 31) * W + (e % W);
+// SELL position of entry e of row i (slices of C rows, chunks of W per lane)
+__device__ __forceinline__ int64_t sell_pos(const int64_t* off, int W, int C, int i, int e) {
+    return off[i / C] + (int64_t)(e / W) * C * W + (i % C) * W + (e % W);
 }
 
 // indices of the SELL copy; a padding slot repeats an index of its own row (or of the
 // slice's first, longest row), so padding stays inside the row's neighbourhood of the
 // gathered vector (its value is 0)
 __global__ void k_sell_idx(int rows, const int32_t* __restrict__ ptr, const int32_t* __restrict__ idx,
-                           const int64_t* __restrict__ off, int W, int32_t* __restrict__ sidx) {
+                           const int64_t* __restrict__ off, int W, int C, int32_t* __restrict__ sidx) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < rows; i += gridDim.x * blockDim.x) {
         const int k0 = ptr[i], len = ptr[i + 1] - k0;
-        const int s = i >> 5;
-        const int plen = (int)((off[s + 1] - off[s]) >> 5);
-        for (int e = 0; e < len; ++e) sidx[sell_pos(off, W, i, e)] = idx[k0 + e];
+        const int s = i / C;
+        const int plen = (int)((off[s + 1] - off[s]) / C);
+        for (int e = 0; e < len; ++e) sidx[sell_pos(off, W, C, i, e)] = idx[k0 + e];
         if (plen > len) {
-            const int first = ptr[s * 32];
-            const int pad = len > 0 ? idx[k0 + len - 1] : (ptr[s * 32 + 1] > first ? idx[first] : 0);
-            for (int e = len; e < plen; ++e) sidx[sell_pos(off, W, i, e)] = pad;
+            const int first = ptr[s * C];
+            const int pad = len > 0 ? idx[k0 + len - 1] : (ptr[s * C + 1] > first ? idx[first] : 0);
+            for (int e = len; e < plen; ++e) sidx[sell_pos(off, W, C, i, e)] = pad;
         }
     }
 }
@@ -755,10 +771,10 @@ __global__ void k_win_setup(int rows, const int32_t* __restrict__ ptr, const int
 
 template <typename VT>
 __global__ void k_sell_vals(int rows, const int32_t* __restrict__ ptr, const double* __restrict__ v64,
-                            const int64_t* __restrict__ off, int W, VT* __restrict__ sval) {
+                            const int64_t* __restrict__ off, int W, int C, VT* __restrict__ sval) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < rows; i += gridDim.x * blockDim.x) {
         const int k0 = ptr[i], len = ptr[i + 1] - k0;
-        for (int e = 0; e < len; ++e) sval[sell_pos(off, W, i, e)] = (VT)v64[k0 + e];
+        for (int e = 0; e < len; ++e) sval[sell_pos(off, W, C, i, e)] = (VT)v64[k0 + e];
     }
 }
 
@@ -1180,7 +1196,9 @@ int build_internal(Ctx* ctx, HalpernWork* w) {
     I.mean_col_len = U.mean_col_len;
     I.max_row_len = U.max_row_len;
     I.max_col_len = U.max_col_len;
-    w->sr.idx_ready = w->sc.idx_ready = false;
+    for (int k = 0; k < 3; ++k) w->sr_all[k].idx_ready = w->sc_all[k].idx_ready = false;
+    w->sr = &w->sr_all[0];
+    w->sc = &w->sc_all[0];
     B2P_CUDA(ctx, cudaStreamSynchronize(s));
     w->ilp_gen = ctx->lp_gen;
     return B2P_OK;
@@ -1189,19 +1207,19 @@ int build_internal(Ctx* ctx, HalpernWork* w) {
 // Slice layout and indices of a SELL copy (once per upload): vector width W = 4 or 2
 // when its padding costs at most 3 % over W = 1, which pads only to each slice's
 // longest row.
-int build_sell_layout(Ctx* ctx, Sell& S, int rows, const int32_t* ptr, const int32_t* idx) {
+int build_sell_layout(Ctx* ctx, Sell& S, int rows, const int32_t* ptr, const int32_t* idx, int C) {
     cudaStream_t s = ctx->stream;
-    const int nsl = (rows + 31) / 32;
+    const int nsl = (rows + C - 1) / C;
     DBuf<int32_t> slen;
     B2P_CUDA(ctx, slen.reserve(nsl));
-    k_slice_len<<<grid_for(nsl, TB, ctx->sm_count), TB, 0, s>>>(rows, ptr, slen.p);
+    k_slice_len<<<grid_for(nsl, TB, ctx->sm_count), TB, 0, s>>>(rows, ptr, C, slen.p);
     B2P_LAUNCH(ctx);
     std::vector<int32_t> h(nsl);
     B2P_CUDA(ctx, cudaMemcpyAsync(h.data(), slen.p, sizeof(int32_t) * nsl, cudaMemcpyDeviceToHost, s));
     B2P_CUDA(ctx, cudaStreamSynchronize(s));
     auto padded_total = [&](int W) {
         int64_t t = 0;
-        for (int v : h) t += 32LL * ((v + W - 1) / W * W);
+        for (int v : h) t += (int64_t)C * ((v + W - 1) / W * W);
         return t;
     };
     const int pad_pct = 3;  // padding allowed for the wider vectors, percent of the W = 1 layout
@@ -1210,7 +1228,8 @@ int build_sell_layout(Ctx* ctx, Sell& S, int rows, const int32_t* ptr, const int
     if (padded_total(4) <= t1 + t1 * pad_pct / 100) W = 4;
     else if (padded_total(2) <= t1 + t1 * pad_pct / 100) W = 2;
     std::vector<int64_t> off(nsl + 1, 0);
-    for (int i = 0; i < nsl; ++i) off[i + 1] = off[i] + 32LL * ((h[i] + W - 1) / W * W);
+    for (int i = 0; i < nsl; ++i) off[i + 1] = off[i] + (int64_t)C * ((h[i] + W - 1) / W * W);
+    S.C = C;
     S.W = W;
     S.slices = nsl;
     S.total = off[nsl];
@@ -1218,7 +1237,7 @@ int build_sell_layout(Ctx* ctx, Sell& S, int rows, const int32_t* ptr, const int
     B2P_CUDA(ctx, S.idx.reserve(std::max<int64_t>(S.total, 1)));
     B2P_CUDA(ctx, cudaMemcpyAsync(S.off.p, off.data(), sizeof(int64_t) * (nsl + 1), cudaMemcpyHostToDevice, s));
     B2P_CUDA(ctx, cudaMemsetAsync(S.idx.p, 0, sizeof(int32_t) * std::max<int64_t>(S.total, 1), s));
-    k_sell_idx<<<grid_for(rows, TB, ctx->sm_count), TB, 0, s>>>(rows, ptr, idx, S.off.p, W, S.idx.p);
+    k_sell_idx<<<grid_for(rows, TB, ctx->sm_count), TB, 0, s>>>(rows, ptr, idx, S.off.p, W, C, S.idx.p);
     B2P_LAUNCH(ctx);
     ctx->launches += 2;
     B2P_CUDA(ctx, cudaStreamSynchronize(s));  // slen is freed on return, h / off are host temporaries
@@ -1236,7 +1255,7 @@ int fill_sell_vals(Ctx* ctx, Sell& S, int rows, const int32_t* ptr, const double
     const bool fresh = out.p == nullptr;
     B2P_CUDA(ctx, out.reserve(std::max<int64_t>(S.total, 1)));
     if (fresh) B2P_CUDA(ctx, cudaMemsetAsync(out.p, 0, sizeof(VT) * std::max<int64_t>(S.total, 1), s));
-    k_sell_vals<VT><<<grid_for(rows, TB, ctx->sm_count), TB, 0, s>>>(rows, ptr, v64, S.off.p, S.W, out.p);
+    k_sell_vals<VT><<<grid_for(rows, TB, ctx->sm_count), TB, 0, s>>>(rows, ptr, v64, S.off.p, S.W, S.C, out.p);
     B2P_LAUNCH(ctx);
     ctx->launches += 1;
     return B2P_OK;
@@ -1299,9 +1318,9 @@ IterArgs<MT, double> primal_args(const DevLP& L, HalpernWork* w, const b2p_param
                            p->reflection, nullptr};
     if (sell) {
         a.ptr = nullptr;
-        a.idx = w->sc.idx.p;
-        a.val = Ops<MT>::sell(w->sc).p;
-        a.soff = w->sc.off.p;
+        a.idx = w->sc->idx.p;
+        a.val = Ops<MT>::sell(*w->sc).p;
+        a.soff = w->sc->off.p;
         a.win_lo = w->wc.lo.p;
         a.win_len = w->wc.len.p;
     }
@@ -1314,9 +1333,9 @@ IterArgs<MT, MT> dual_args(const DevLP& L, HalpernWork* w, const b2p_params* p, 
                        p->reflection, nullptr};
     if (sell) {
         a.ptr = nullptr;
-        a.idx = w->sr.idx.p;
-        a.val = Ops<MT>::sell(w->sr).p;
-        a.soff = w->sr.off.p;
+        a.idx = w->sr->idx.p;
+        a.val = Ops<MT>::sell(*w->sr).p;
+        a.soff = w->sr->off.p;
         a.win_lo = w->wr.lo.p;
         a.win_len = w->wr.len.p;
     }
@@ -1327,43 +1346,51 @@ IterArgs<MT, MT> dual_args(const DevLP& L, HalpernWork* w, const b2p_params* p, 
 // windowed instantiation is opened up to it once per process.
 constexpr int kWinSmemMax = 200 * 1024;
 
-template <typename VT, typename GT, int W, int MODE, bool PRIMAL, bool WIN>
+template <typename VT, typename GT, int W, int C, int MODE, bool PRIMAL, bool WIN>
 void launch_sell_one(unsigned grid, int tb, size_t smem, cudaStream_t s, const IterArgs<VT, GT>& a, int it) {
     if (WIN) {
         static unsigned long long opened = 0;  // host-side, per instantiation: one bit per device
         int dev = 0;
         cudaGetDevice(&dev);
         if (dev < 64 && !((opened >> dev) & 1ull)) {
-            cudaFuncSetAttribute(k_iter_sell<VT, GT, W, MODE, PRIMAL, WIN>,
+            cudaFuncSetAttribute(k_iter_sell<VT, GT, W, C, MODE, PRIMAL, WIN>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, kWinSmemMax);
             opened |= 1ull << dev;
         }
     }
-    k_iter_sell<VT, GT, W, MODE, PRIMAL, WIN><<<grid, tb, WIN ? smem : 0, s>>>(a, it);
+    k_iter_sell<VT, GT, W, C, MODE, PRIMAL, WIN><<<grid, tb, WIN ? smem : 0, s>>>(a, it);
 }
 
-template <typename VT, typename GT, int MODE, bool PRIMAL, bool WIN>
+template <typename VT, typename GT, int C, int MODE, bool PRIMAL, bool WIN>
 void launch_sell_W(int W, unsigned grid, int tb, size_t smem, cudaStream_t s, const IterArgs<VT, GT>& a, int it) {
     switch (W) {
-        case 4: launch_sell_one<VT, GT, 4, MODE, PRIMAL, WIN>(grid, tb, smem, s, a, it); break;
-        case 2: launch_sell_one<VT, GT, 2, MODE, PRIMAL, WIN>(grid, tb, smem, s, a, it); break;
-        default: launch_sell_one<VT, GT, 1, MODE, PRIMAL, WIN>(grid, tb, smem, s, a, it); break;
+        case 4: launch_sell_one<VT, GT, 4, C, MODE, PRIMAL, WIN>(grid, tb, smem, s, a, it); break;
+        case 2: launch_sell_one<VT, GT, 2, C, MODE, PRIMAL, WIN>(grid, tb, smem, s, a, it); break;
+        default: launch_sell_one<VT, GT, 1, C, MODE, PRIMAL, WIN>(grid, tb, smem, s, a, it); break;
     }
 }
 
-// smem > 0: windowed variant (a.win_lo / a.win_len set for this grid), else plain SELL
-template <typename VT, typename GT, bool PRIMAL>
-void launch_sell(int mode, int W, unsigned grid, int tb, size_t smem, cudaStream_t s, const IterArgs<VT, GT>& a,
-                 int it) {
-    if (smem > 0) {
-        if (mode == M_FIRST) launch_sell_W<VT, GT, M_FIRST, PRIMAL, true>(W, grid, tb, smem, s, a, it);
-        else if (mode == M_CHECK) launch_sell_W<VT, GT, M_CHECK, PRIMAL, true>(W, grid, tb, smem, s, a, it);
-        else launch_sell_W<VT, GT, M_PLAIN, PRIMAL, true>(W, grid, tb, smem, s, a, it);
-    } else {
-        if (mode == M_FIRST) launch_sell_W<VT, GT, M_FIRST, PRIMAL, false>(W, grid, tb, 0, s, a, it);
-        else if (mode == M_CHECK) launch_sell_W<VT, GT, M_CHECK, PRIMAL, false>(W, grid, tb, 0, s, a, it);
-        else launch_sell_W<VT, GT, M_PLAIN, PRIMAL, false>(W, grid, tb, 0, s, a, it);
+template <typename VT, typename GT, int MODE, bool PRIMAL>
+void launch_sell_CW(const Sell& S, unsigned grid, int tb, size_t smem, cudaStream_t s, const IterArgs<VT, GT>& a,
+                    int it) {
+    if (smem > 0) {  // gather windows: 32-row slices only
+        launch_sell_W<VT, GT, 32, MODE, PRIMAL, true>(S.W, grid, tb, smem, s, a, it);
+        return;
     }
+    switch (S.C) {
+        case 8: launch_sell_W<VT, GT, 8, MODE, PRIMAL, false>(S.W, grid, tb, 0, s, a, it); break;
+        case 16: launch_sell_W<VT, GT, 16, MODE, PRIMAL, false>(S.W, grid, tb, 0, s, a, it); break;
+        default: launch_sell_W<VT, GT, 32, MODE, PRIMAL, false>(S.W, grid, tb, 0, s, a, it); break;
+    }
+}
+
+// smem > 0: windowed variant (a.win_lo / a.win_len set for this grid; S.C == 32), else plain SELL
+template <typename VT, typename GT, bool PRIMAL>
+void launch_sell(int mode, const Sell& S, unsigned grid, int tb, size_t smem, cudaStream_t s,
+                 const IterArgs<VT, GT>& a, int it) {
+    if (mode == M_FIRST) launch_sell_CW<VT, GT, M_FIRST, PRIMAL>(S, grid, tb, smem, s, a, it);
+    else if (mode == M_CHECK) launch_sell_CW<VT, GT, M_CHECK, PRIMAL>(S, grid, tb, smem, s, a, it);
+    else launch_sell_CW<VT, GT, M_PLAIN, PRIMAL>(S, grid, tb, smem, s, a, it);
 }
 
 // One resident wave: 2048 / tb CTAs per SM, each owning a contiguous row range.
@@ -1382,9 +1409,9 @@ int sell_win_per_sm(int W, int tb, size_t smem) {
         cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, kWinSmemMax);
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, tb, smem);
     };
-    if (W == 4) q(k_iter_sell<VT, GT, 4, M_PLAIN, PRIMAL, true>);
-    else if (W == 2) q(k_iter_sell<VT, GT, 2, M_PLAIN, PRIMAL, true>);
-    else q(k_iter_sell<VT, GT, 1, M_PLAIN, PRIMAL, true>);
+    if (W == 4) q(k_iter_sell<VT, GT, 4, 32, M_PLAIN, PRIMAL, true>);
+    else if (W == 2) q(k_iter_sell<VT, GT, 2, 32, M_PLAIN, PRIMAL, true>);
+    else q(k_iter_sell<VT, GT, 1, 32, M_PLAIN, PRIMAL, true>);
     return per;
 }
 
@@ -1396,30 +1423,55 @@ int side_windows(Ctx* ctx, HalpernWork* w, bool primal, int k) {
     const size_t smem = kWinShapes[k][1];
     if (primal)
         return build_windows(ctx, w->wc, L.n, L.t_rowptr.p, L.t_colidx.p, L.m, tb, smem, sizeof(double),
-                             sell_win_per_sm<MT, double, true>(w->sc.W, tb, smem));
+                             sell_win_per_sm<MT, double, true>(w->sc_all[0].W, tb, smem));
     return build_windows(ctx, w->wr, L.m, L.rowptr.p, L.colidx.p, L.n, tb, smem, sizeof(MT),
-                         sell_win_per_sm<MT, MT, false>(w->sr.W, tb, smem));
+                         sell_win_per_sm<MT, MT, false>(w->sr_all[0].W, tb, smem));
+}
+
+// Slice heights of the SELL layouts (index k of sr_all / sc_all).
+constexpr int kSliceC[3] = {32, 16, 8};
+
+// SELL layout k of one side with the current solve's scaled values (built on first use).
+template <typename MT>
+int ensure_sell(Ctx* ctx, HalpernWork* w, bool primal, int k) {
+    const DevLP& L = w->ilp;
+    Sell& S = primal ? w->sc_all[k] : w->sr_all[k];
+    if (S.idx_ready) return B2P_OK;
+    int st = primal ? build_sell_layout(ctx, S, L.n, L.t_rowptr.p, L.t_colidx.p, kSliceC[k])
+                    : build_sell_layout(ctx, S, L.m, L.rowptr.p, L.colidx.p, kSliceC[k]);
+    if (st) return st;
+    return primal ? fill_sell_vals<MT>(ctx, S, L.n, L.t_rowptr.p, w->stv64.p, Ops<MT>::sell(S))
+                  : fill_sell_vals<MT>(ctx, S, L.m, L.rowptr.p, w->sv64.p, Ops<MT>::sell(S));
 }
 
 // Times candidate launch shapes of the primal and dual kernels on the uploaded LP
 // (plain iterations from the current iterates, CUDA events on the context stream)
-// and keeps the fastest of each side: the SELL kernel with CTA sizes 256 / 512 /
-// 1024, the SELL kernel with gather windows in shared memory (kWinShapes), and the
-// CSR kernel with (L lanes per row, R rows per lane group, CTA size).  The caller
+// and keeps the fastest of each side: the SELL kernel with slice heights 32 / 16 / 8
+// (1 / 2 / 4 lanes per row) and CTA sizes 256 / 512 / 1024, the SELL kernel with
+// gather windows in shared memory (32-row slices, kWinShapes), and the CSR kernel
+// with (L lanes per row, R rows per lane group, CTA size).  The caller
 // re-initialises the iterates afterwards.  lanes_per_row > 0 forces the CSR kernel
-// with that L, -1 the SELL kernel (CTA size 256), -2 the windowed SELL kernel (CTA
-// size 512, 96 KB); each skips the search.
+// with that L, -1 the SELL kernel (32-row slices, CTA size 256), -2 the windowed
+// SELL kernel (CTA size 512, 96 KB), -3 / -4 the SELL kernel with 16- / 8-row slices
+// (CTA size 256); each skips the search.
 template <typename MT>
 int autotune_shapes(Ctx* ctx, HalpernWork* w, const b2p_params* p) {
     DevLP& L = w->ilp;
     const long long key = ((long long)L.nnz * 1000003LL + (long long)L.m * 101LL + L.n) * 2 + (sizeof(MT) == 4);
     if (p->lanes_per_row != 0) {
         const bool sell = p->lanes_per_row < 0;
+        const int k = p->lanes_per_row == -3 ? 1 : (p->lanes_per_row == -4 ? 2 : 0);
         w->sell_c = w->sell_r = sell;
-        w->Lc = w->Lr = sell ? 1 : pick_lanes(0, p->lanes_per_row);
+        w->Lc = w->Lr = sell ? 32 / kSliceC[k] : pick_lanes(0, p->lanes_per_row);
         w->Rc = w->Rr = 1;
         w->Tc = w->Tr = 256;
         w->wc.smem = w->wr.smem = 0;
+        for (int side = 0; side < 2 && sell; ++side) {
+            int st = ensure_sell<MT>(ctx, w, side == 0, k);
+            if (st) return st;
+        }
+        w->sc = &w->sc_all[k];
+        w->sr = &w->sr_all[k];
         if (p->lanes_per_row == -2) {
             w->Tc = w->Tr = kWinShapes[1][0];
             for (int side = 0; side < 2; ++side) {
@@ -1442,30 +1494,39 @@ int autotune_shapes(Ctx* ctx, HalpernWork* w, const b2p_params* p) {
         const double mean = primal ? L.mean_col_len : L.mean_row_len;
         const int base_L = pick_lanes(mean, 0);
         Win& win = primal ? w->wc : w->wr;
+        Sell** cur = primal ? &w->sc : &w->sr;
+        Sell* all = primal ? w->sc_all : w->sr_all;
         float best = 1e30f;
-        int bestL = base_L, bestR = 1, bestT = 256, bestWin = -1;
+        int bestL = base_L, bestR = 1, bestT = 256, bestWin = -1, bestK = 0;
         bool bestS = false;
-        // kind 0: CSR (Lc, R, tb); 1: SELL (tb); 2: windowed SELL (shape k)
+        // kind 0: CSR (Lc, R, tb); 1: SELL (layout k, tb); 2: windowed SELL (32-row slices, shape k)
         auto trial = [&](int kind, int Lc, int R, int tb, int k) -> int {
             unsigned g;
             size_t smem = 0;
             if (kind == 2) {
+                *cur = &all[0];
                 int st = side_windows<MT>(ctx, w, primal, k);
                 if (st) return st;
                 if (win.smem == 0) return B2P_OK;  // not possible for this LP
                 g = win.G;
                 smem = win.smem;
+            } else if (kind == 1) {
+                int st = ensure_sell<MT>(ctx, w, primal, k);
+                if (st) return st;
+                *cur = &all[k];
+                win.smem = 0;
+                g = iter_grid(rows, 32 / kSliceC[k], 1, tb, ctx->sm_count);
             } else {
                 win.smem = 0;
-                g = kind == 1 ? iter_grid(rows, 1, 1, tb, ctx->sm_count) : iter_grid(rows, Lc, R, tb, ctx->sm_count);
+                g = iter_grid(rows, Lc, R, tb, ctx->sm_count);
             }
             const IterArgs<MT, double> pa = primal_args<MT>(L, w, p, kind != 0);
             const IterArgs<MT, MT> da = dual_args<MT>(L, w, p, kind != 0);
             float tot = 0.f;
             for (int rep = 0; rep < 4; ++rep) {
                 cudaEventRecord(e0, s);
-                if (kind != 0 && primal) launch_sell<MT, double, true>(M_PLAIN, w->sc.W, g, tb, smem, s, pa, rep);
-                else if (kind != 0) launch_sell<MT, MT, false>(M_PLAIN, w->sr.W, g, tb, smem, s, da, rep);
+                if (kind != 0 && primal) launch_sell<MT, double, true>(M_PLAIN, **cur, g, tb, smem, s, pa, rep);
+                else if (kind != 0) launch_sell<MT, MT, false>(M_PLAIN, **cur, g, tb, smem, s, da, rep);
                 else if (primal) launch_iter<MT, double, true>(M_PLAIN, Lc, R, g, tb, s, pa, rep);
                 else launch_iter<MT, MT, false>(M_PLAIN, Lc, R, g, tb, s, da, rep);
                 cudaEventRecord(e1, s);
@@ -1480,16 +1541,18 @@ int autotune_shapes(Ctx* ctx, HalpernWork* w, const b2p_params* p) {
                 best = tot;
                 bestS = kind != 0;
                 bestWin = kind == 2 ? k : -1;
-                bestL = Lc;
+                bestK = kind == 1 ? k : 0;
+                bestL = kind == 1 ? 32 / kSliceC[k] : Lc;
                 bestR = R;
                 bestT = tb;
             }
             return B2P_OK;
         };
-        for (int tb : {256, 512, 1024}) {
-            int st = trial(1, 1, 1, tb, 0);
-            if (st) return st;
-        }
+        for (int k = 0; k < 3; ++k)
+            for (int tb : {256, 512, 1024}) {
+                int st = trial(1, 1, 1, tb, k);
+                if (st) return st;
+            }
         for (int k = 0; k < 3; ++k) {
             int st = trial(2, 1, 1, kWinShapes[k][0], k);
             if (st) return st;
@@ -1503,6 +1566,7 @@ int autotune_shapes(Ctx* ctx, HalpernWork* w, const b2p_params* p) {
                 }
         }
         win.smem = 0;
+        *cur = &all[bestK];
         if (bestWin >= 0) {
             int st = side_windows<MT>(ctx, w, primal, bestWin);
             if (st) return st;
@@ -1535,10 +1599,10 @@ int run_chunks(Ctx* ctx, HalpernWork* w, const b2p_params* p, double time_limit_
     auto chunk = [&]() {
         for (int i = 0; i < K; ++i) {
             int mode = (i == 0) ? M_FIRST : (i == K - 1 ? M_CHECK : M_PLAIN);
-            if (w->sell_c) launch_sell<MT, double, true>(mode, w->sc.W, gcS, Tc, w->wc.smem, s, pa, i);
+            if (w->sell_c) launch_sell<MT, double, true>(mode, *w->sc, gcS, Tc, w->wc.smem, s, pa, i);
             else if (mode == M_PLAIN) launch_iter<MT, double, true>(mode, Lc, Rc, gcR, Tc, s, pa, i);
             else launch_iter<MT, double, true>(mode, Lc, 1, gc, Tc, s, pa, i);
-            if (w->sell_r) launch_sell<MT, MT, false>(mode, w->sr.W, grS, Tr, w->wr.smem, s, da, i);
+            if (w->sell_r) launch_sell<MT, MT, false>(mode, *w->sr, grS, Tr, w->wr.smem, s, da, i);
             else if (mode == M_PLAIN) launch_iter<MT, MT, false>(mode, Lr, Rr, grR, Tr, s, da, i);
             else launch_iter<MT, MT, false>(mode, Lr, 1, gr, Tr, s, da, i);
         }
@@ -1643,18 +1707,28 @@ int solve_T(Ctx* ctx, HalpernWork* w, const b2p_params* p, const double* x0, con
     }
     int st = prepare_scaling(ctx, w, p->ruiz_iterations, mixed);
     if (st) return st;
-    if (!w->sr.idx_ready) {
-        st = build_sell_layout(ctx, w->sr, m, L.rowptr.p, L.colidx.p);
-        if (st) return st;
+    // SELL layouts: the 32-row one always, the others once the tuner has built them;
+    // every built layout gets this solve's scaled values
+    for (int k = 0; k < 3; ++k) {
+        Sell& R = w->sr_all[k];
+        Sell& Cc = w->sc_all[k];
+        if (k == 0 && !R.idx_ready) {
+            st = build_sell_layout(ctx, R, m, L.rowptr.p, L.colidx.p, kSliceC[0]);
+            if (st) return st;
+        }
+        if (k == 0 && !Cc.idx_ready) {
+            st = build_sell_layout(ctx, Cc, n, L.t_rowptr.p, L.t_colidx.p, kSliceC[0]);
+            if (st) return st;
+        }
+        if (R.idx_ready) {
+            st = fill_sell_vals<MT>(ctx, R, m, L.rowptr.p, w->sv64.p, Ops<MT>::sell(R));
+            if (st) return st;
+        }
+        if (Cc.idx_ready) {
+            st = fill_sell_vals<MT>(ctx, Cc, n, L.t_rowptr.p, w->stv64.p, Ops<MT>::sell(Cc));
+            if (st) return st;
+        }
     }
-    if (!w->sc.idx_ready) {
-        st = build_sell_layout(ctx, w->sc, n, L.t_rowptr.p, L.t_colidx.p);
-        if (st) return st;
-    }
-    st = fill_sell_vals<MT>(ctx, w->sr, m, L.rowptr.p, w->sv64.p, Ops<MT>::sell(w->sr));
-    if (st) return st;
-    st = fill_sell_vals<MT>(ctx, w->sc, n, L.t_rowptr.p, w->stv64.p, Ops<MT>::sell(w->sc));
-    if (st) return st;
     double sig2 = 0.0;
     st = power_sigma2(ctx, w, &sig2);
     if (st) return st;
@@ -1797,10 +1871,10 @@ int kernel_timing_T(Ctx* ctx, HalpernWork* w, const b2p_params* p, int reps, dou
     double tp = 0, td = 0;
     for (int r = 0; r < reps; ++r) {
         cudaEventRecord(e[0], s);
-        if (w->sell_c) launch_sell<MT, double, true>(M_PLAIN, w->sc.W, gc, Tc, w->wc.smem, s, pa, r);
+        if (w->sell_c) launch_sell<MT, double, true>(M_PLAIN, *w->sc, gc, Tc, w->wc.smem, s, pa, r);
         else launch_iter<MT, double, true>(M_PLAIN, Lc, Rc, gc, Tc, s, pa, r);
         cudaEventRecord(e[1], s);
-        if (w->sell_r) launch_sell<MT, MT, false>(M_PLAIN, w->sr.W, gr, Tr, w->wr.smem, s, da, r);
+        if (w->sell_r) launch_sell<MT, MT, false>(M_PLAIN, *w->sr, gr, Tr, w->wr.smem, s, da, r);
         else launch_iter<MT, MT, false>(M_PLAIN, Lr, Rr, gr, Tr, s, da, r);
         cudaEventRecord(e[2], s);
         B2P_LAUNCH(ctx);
@@ -1820,8 +1894,8 @@ int kernel_timing_T(Ctx* ctx, HalpernWork* w, const b2p_params* p, int reps, dou
     // algorithmic bytes: every matrix entry, row pointer (CSR) or slice offset (SELL) and
     // vector element once; SELL padding is not counted
     const double vb = sizeof(MT), nnz = (double)L.nnz;
-    const double pc_bytes = w->sell_c ? 8.0 * (w->sc.slices + 1) : 4.0 * (n + 1);
-    const double pr_bytes = w->sell_r ? 8.0 * (w->sr.slices + 1) : 4.0 * (m + 1);
+    const double pc_bytes = w->sell_c ? 8.0 * (w->sc->slices + 1) : 4.0 * (n + 1);
+    const double pr_bytes = w->sell_r ? 8.0 * (w->sr->slices + 1) : 4.0 * (m + 1);
     // primal: A^T values+indices, col pointers, gather y (m x 8), x r/w, xa, c, l, u (8 each), xh write
     *pb = nnz * (vb + 4) + pc_bytes + 8.0 * m + n * (8 * 6 + vb);
     // dual: A values+indices, row pointers, gather xh (n x vb), y r/w, ya, b (8 each), is_eq (1)

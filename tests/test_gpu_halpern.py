@@ -144,17 +144,18 @@ def test_mixed_without_refinement_matches_fp64_iterations_at_1e6(ctx, lps):
     assert abs(r64["iterations"] - r32["iterations"]) <= 2 * 64
 
 
-KERNELS = {"sell": -1, "sell_window": -2, "csr": 8}
+KERNELS = {"sell": -1, "sell_window": -2, "sell16": -3, "sell8": -4, "csr": 8}
 
 
 @pytest.mark.parametrize("precision", ["fp64", "fp32"])
 @pytest.mark.parametrize("kernel", list(KERNELS))
 @pytest.mark.parametrize("name", ["rs_c0", "ba_tiny", "ill_small"])
 def test_iteration_kernel_variants(ctx, golden, lps, name, precision, kernel):
-    """Every iteration kernel -- SELL-32 over the length-sorted internal numbering
-    (lanes_per_row = -1), the same with per-CTA gather windows in shared memory (-2),
-    and sub-warp CSR (8) -- reaches the tolerance, and the answer, mapped back to the
-    caller's numbering, matches the oracle's KKT and the HiGHS optimum."""
+    """Every iteration kernel -- SELL over the length-sorted internal numbering with
+    32-row slices (lanes_per_row = -1), the same with per-CTA gather windows in shared
+    memory (-2), 16- and 8-row slices with 2 / 4 lanes per row (-3, -4), and sub-warp
+    CSR (8) -- reaches the tolerance, and the answer, mapped back to the caller's
+    numbering, matches the oracle's KKT and the HiGHS optimum."""
     std = lps[name].standard()
     ctx.upload(std)
     eps = 1e-8 if name == "ill_small" else 1e-6
@@ -175,7 +176,7 @@ def test_sell_and_csr_agree_on_iterates(ctx, lps):
     std = lps["ba_tiny"].standard()
     ctx.upload(std)
     rb, xb, yb = ctx.solve(engine="halpern", precision="fp64", eps=0.0, max_iterations=512, lanes_per_row=8)
-    for lpr in (-1, -2):
+    for lpr in (-1, -2, -3, -4):
         ra, xa, ya = ctx.solve(engine="halpern", precision="fp64", eps=0.0, max_iterations=512, lanes_per_row=lpr)
         assert ra["iterations"] == rb["iterations"] == 512
         assert np.allclose(xa, xb, rtol=1e-9, atol=1e-9 * (1 + np.abs(xb).max()))
