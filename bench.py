@@ -12,10 +12,12 @@ one batched solve of all held-out instances; N GPUs run N replicas on their own
 held-out seeds (weak scaling).
 
 Other workloads: block_angular (single 204k x 1M LP), random_sparse (300 x 1000),
-uneven_batch (4096 independent LPs), refinery (random-structure family, cold).
+uneven_batch (4096 independent LPs), refinery (random-structure family, cold),
+ill_conditioned (single 1M x 5M LP, 50M nonzeros, badly scaled; to 1e-8 by default,
+each solve takes minutes: use --steps 1 --e2e-steps 0).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                  [--workload refinery_learned|block_angular|uneven_batch|refinery|random_sparse]
+                  [--workload refinery_learned|block_angular|uneven_batch|refinery|random_sparse|ill_conditioned]
 """
 from __future__ import annotations
 
@@ -39,7 +41,9 @@ sys.path.insert(0, str(ROOT))
 # extrapolates the reference CPU solver's per-iteration cost over this many
 # iterations -- generous to the CPU: the reference's own vanilla PDHG needs far
 # more iterations and never reaches 1e-6 on these LPs.
-HALPERN_ITERS = {"block_angular": 6784, "random_sparse": 5056, "refinery_learned": 65388}
+HALPERN_ITERS = {"block_angular": 6784, "random_sparse": 5056, "refinery_learned": 65388,
+                 # mixed engine to 1e-8 (the FP64 leg of this workload was not run)
+                 "ill_conditioned": 1230784}
 
 METRIC = "LPs/sec to 1e-6 rel KKT"
 
