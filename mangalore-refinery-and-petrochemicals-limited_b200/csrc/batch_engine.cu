@@ -257,8 +257,12 @@ __device__ void rebuild_shifted(const BArgs& a, int m, int n, int64_t ro, int64_
     }
 }
 
+// Body of the persistent chunk kernel; launched as k_batch_chunk (the tuned CTA
+// size, up to 512 threads, two CTAs per SM) while many instances are active and as
+// k_batch_chunk_wide (1024 threads, one CTA per SM) once no more than one instance
+// per SM is left, so the last, slowest instances iterate with twice the threads.
 template <typename MT>
-__global__ void __launch_bounds__(512, 2) k_batch_chunk(BArgs a, int chunk) {
+__device__ __forceinline__ void batch_chunk_body(BArgs a, int chunk) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ double red[32 * 6];
     __shared__ InstCtrl sc;
@@ -521,6 +525,16 @@ __global__ void __launch_bounds__(512, 2) k_batch_chunk(BArgs a, int chunk) {
         }
         __syncthreads();
     }
+}
+
+template <typename MT>
+__global__ void __launch_bounds__(512, 2) k_batch_chunk(BArgs a, int chunk) {
+    batch_chunk_body<MT>(a, chunk);
+}
+
+template <typename MT>
+__global__ void __launch_bounds__(1024, 1) k_batch_chunk_wide(BArgs a, int chunk) {
+    batch_chunk_body<MT>(a, chunk);
 }
 
 // Order-preserving compaction of the active list (one CTA).
@@ -1122,24 +1136,38 @@ int batch_run(Ctx* ctx, BatchWork* w, const b2p_params* p, const double* x0_dev,
     const int grid = ctx->sm_count * per_sm;
     BArgs a1 = make_args<MT>(w, p, w->active.p);
     BArgs a2 = make_args<MT>(w, p, w->active2.p);
-    // one graph = two chunk launches with compaction (ping-pong active lists)
-    cudaGraph_t graph = nullptr;
-    cudaGraphExec_t exec = nullptr;
-    B2P_CUDA(ctx, cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
-    fn<<<grid, cfg.threads, sm, s>>>(a1, cfg.chunk);
-    k_batch_compact<<<1, 1024, 0, s>>>(w->ictrl.p, w->active.p, w->active2.p, w->counters.p);
-    fn<<<grid, cfg.threads, sm, s>>>(a2, cfg.chunk);
-    k_batch_compact<<<1, 1024, 0, s>>>(w->ictrl.p, w->active2.p, w->active.p, w->counters.p);
-    cudaError_t ce = cudaStreamEndCapture(s, &graph);
-    if (ce != cudaSuccess) {
-        ctx->err = std::string("batch graph capture: ") + cudaGetErrorString(ce);
-        return B2P_EXECUTION_FAILED;
-    }
-    ce = cudaGraphInstantiate(&exec, graph, 0);
-    if (ce != cudaSuccess) {
-        cudaGraphDestroy(graph);
-        ctx->err = std::string("batch graph instantiate: ") + cudaGetErrorString(ce);
-        return B2P_EXECUTION_FAILED;
+    // the wide form for the tail: 1024 threads, one CTA per SM
+    auto fnw = k_batch_chunk_wide<MT>;
+    B2P_CUDA(ctx, cudaFuncSetAttribute(fnw, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    int per_sm_w = 0;
+    B2P_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_w, fnw, 1024, sm));
+    const bool have_wide = per_sm_w >= 1;
+    const int grid_w = ctx->sm_count * std::max(per_sm_w, 1);
+    // one graph = two chunk launches with compaction (ping-pong active lists); a second
+    // graph does the same with the wide kernel
+    cudaGraph_t graph = nullptr, graph_w = nullptr;
+    cudaGraphExec_t exec = nullptr, exec_w = nullptr;
+    for (int g = 0; g < (have_wide ? 2 : 1); ++g) {
+        B2P_CUDA(ctx, cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+        if (g == 0) fn<<<grid, cfg.threads, sm, s>>>(a1, cfg.chunk);
+        else fnw<<<grid_w, 1024, sm, s>>>(a1, cfg.chunk);
+        k_batch_compact<<<1, 1024, 0, s>>>(w->ictrl.p, w->active.p, w->active2.p, w->counters.p);
+        if (g == 0) fn<<<grid, cfg.threads, sm, s>>>(a2, cfg.chunk);
+        else fnw<<<grid_w, 1024, sm, s>>>(a2, cfg.chunk);
+        k_batch_compact<<<1, 1024, 0, s>>>(w->ictrl.p, w->active2.p, w->active.p, w->counters.p);
+        cudaGraph_t& gr = g == 0 ? graph : graph_w;
+        cudaGraphExec_t& ex = g == 0 ? exec : exec_w;
+        cudaError_t ce = cudaStreamEndCapture(s, &gr);
+        if (ce != cudaSuccess) {
+            ctx->err = std::string("batch graph capture: ") + cudaGetErrorString(ce);
+            return B2P_EXECUTION_FAILED;
+        }
+        ce = cudaGraphInstantiate(&ex, gr, 0);
+        if (ce != cudaSuccess) {
+            cudaGraphDestroy(gr);
+            ctx->err = std::string("batch graph instantiate: ") + cudaGetErrorString(ce);
+            return B2P_EXECUTION_FAILED;
+        }
     }
     int32_t* host_cnt = nullptr;
     B2P_CUDA(ctx, cudaMallocHost(&host_cnt, 2 * sizeof(int32_t)));
@@ -1148,12 +1176,15 @@ int batch_run(Ctx* ctx, BatchWork* w, const b2p_params* p, const double* x0_dev,
     bool timed_out = false;
     const double tl = p->time_limit_s * 1000.0;
     cudaEventRecord(ctx->ev0, s);
+    // no more than one instance per SM left: the wide form
+    bool wide = have_wide && n_act <= ctx->sm_count;
     while (graphs < max_graphs) {
-        B2P_CUDA(ctx, cudaGraphLaunch(exec, s));
+        B2P_CUDA(ctx, cudaGraphLaunch(wide ? exec_w : exec, s));
         graphs++;
         B2P_CUDA(ctx, cudaMemcpyAsync(host_cnt, w->counters.p, 2 * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
         B2P_CUDA(ctx, cudaStreamSynchronize(s));
         if (host_cnt[1] == 0) break;
+        if (have_wide && host_cnt[1] <= ctx->sm_count) wide = true;
         if (tl > 0 && now_ms() - t_start > tl) {
             timed_out = true;
             break;
@@ -1164,6 +1195,10 @@ int batch_run(Ctx* ctx, BatchWork* w, const b2p_params* p, const double* x0_dev,
     cudaFreeHost(host_cnt);
     cudaGraphExecDestroy(exec);
     cudaGraphDestroy(graph);
+    if (have_wide) {
+        cudaGraphExecDestroy(exec_w);
+        cudaGraphDestroy(graph_w);
+    }
     ctx->launches += graphs * 4;
     float kms = 0;
     cudaEventElapsedTime(&kms, ctx->ev0, ctx->ev1);

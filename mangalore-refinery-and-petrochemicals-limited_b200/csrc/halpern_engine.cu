@@ -117,6 +117,9 @@ struct HalpernWork {
     // tuned gather windows of the SELL kernels (smem 0 = none): grid, shared memory
     // bytes and the per-CTA windows built for that grid
     Win wr, wc;
+    // tuned layout index (into sr_all / sc_all) and window shape (-1 = none) per side, so
+    // a later upload of an LP of the same size can rebuild what the tuned shape needs
+    int kr_t = 0, kc_t = 0, winr_t = -1, winc_t = -1;
     int64_t solved_gen = -1;     // upload generation and precision of the last solve
     int solved_precision = -1;   // (the state b2p_kernel_timing replays)
     DBuf<double> dr, dc, tmp_m, tmp_n, pv, pu, pw;
@@ -1482,7 +1485,22 @@ int autotune_shapes(Ctx* ctx, HalpernWork* w, const b2p_params* p) {
         w->tuned_key = -1;
         return B2P_OK;
     }
-    if (w->tuned_key == key) return B2P_OK;
+    if (w->tuned_key == key) {
+        // same size as the tuned LP (possibly another upload): its layouts and windows
+        for (int side = 0; side < 2; ++side) {
+            const bool primal = side == 0;
+            const int k = primal ? w->kc_t : w->kr_t, wk = primal ? w->winc_t : w->winr_t;
+            int st = ensure_sell<MT>(ctx, w, primal, k);
+            if (st) return st;
+            (primal ? w->sc : w->sr) = &(primal ? w->sc_all : w->sr_all)[k];
+            (primal ? w->wc : w->wr).smem = 0;
+            if (wk >= 0) {
+                st = side_windows<MT>(ctx, w, primal, wk);
+                if (st) return st;
+            }
+        }
+        return B2P_OK;
+    }
     cudaStream_t s = ctx->stream;
     const int m = L.m, n = L.n;
     cudaEvent_t e0, e1;
@@ -1571,8 +1589,13 @@ int autotune_shapes(Ctx* ctx, HalpernWork* w, const b2p_params* p) {
             int st = side_windows<MT>(ctx, w, primal, bestWin);
             if (st) return st;
         }
-        if (primal) { w->sell_c = bestS; w->Lc = bestL; w->Rc = bestR; w->Tc = bestT; }
-        else { w->sell_r = bestS; w->Lr = bestL; w->Rr = bestR; w->Tr = bestT; }
+        if (primal) {
+            w->sell_c = bestS; w->Lc = bestL; w->Rc = bestR; w->Tc = bestT;
+            w->kc_t = bestK; w->winc_t = bestWin;
+        } else {
+            w->sell_r = bestS; w->Lr = bestL; w->Rr = bestR; w->Tr = bestT;
+            w->kr_t = bestK; w->winr_t = bestWin;
+        }
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);

@@ -193,3 +193,34 @@ def test_warm_start_is_renumbered(ctx, lps):
     res2, x2, y2 = ctx.solve(x0=x, y0=y, engine="halpern", precision="fp64", eps=1e-6, lanes_per_row=-1,
                              primal_weight=res["primal_weight"])
     assert res2["status"] == "OPTIMAL" and res2["iterations"] <= 128, res2
+
+
+def test_same_size_upload_reuses_tuning_safely(ctx, golden, lps, lpgen):
+    """A second upload of an LP with the same sizes but another structure (the columns
+    of the block-angular LP shuffled) reuses the tuned launch shape; the layouts and
+    gather windows that shape needs are rebuilt for the new matrix, so the answer is
+    right: same optimum, KKT within tolerance."""
+    std = lps["ba_tiny"].standard()
+    ctx.upload(std)
+    r1, x1, y1 = ctx.solve(engine="halpern", precision="fp32", eps=1e-6, max_iterations=400000)
+    assert r1["status"] == "OPTIMAL"
+    rng = np.random.default_rng(5)
+    perm = rng.permutation(std.n)          # new column j = old column perm[j]
+    inv = np.empty_like(perm)
+    inv[perm] = np.arange(std.n)
+    colidx = inv[std.colidx].astype(np.int32)
+    rowptr = std.rowptr.copy()
+    vals = std.vals.copy()
+    for i in range(std.m):                 # keep column indices ascending inside each row
+        a, b = rowptr[i], rowptr[i + 1]
+        o = np.argsort(colidx[a:b])
+        colidx[a:b] = colidx[a:b][o]
+        vals[a:b] = vals[a:b][o]
+    sh = lpgen.StdLP(std.m, std.n, rowptr, colidx, vals, std.b, std.c[perm], std.lb[perm], std.ub[perm], std.is_eq)
+    ctx.upload(sh)
+    r2, x2, y2 = ctx.solve(engine="halpern", precision="fp32", eps=1e-6, max_iterations=400000)
+    assert r2["status"] == "OPTIMAL", r2
+    k = pdlp_oracle.kkt(sh, x2, y2)
+    assert k["rel_kkt"] <= 1.05e-6, k
+    z = golden["highs"]["ba_tiny"]
+    assert abs(k["pobj"] - z) <= 1e-6 * max(1.0, abs(z)), (k["pobj"], z)
