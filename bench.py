@@ -47,6 +47,12 @@ HALPERN_ITERS = {"block_angular": 6784, "random_sparse": 5056, "refinery_learned
 
 METRIC = "LPs/sec to 1e-6 rel KKT"
 
+# Seconds of each part of the refinery_learned run on one B200 (2,000 held-out
+# instances; labels to 1e-8, legs to 1e-6 relative KKT with the answer's objective
+# within 1e-6), used to plan the run's wall time from its leg counts.
+LEARNED_LEG_S = {"start": 30.0, "label_per_instance": 0.0144, "epoch": 0.044, "warmup_step": 2.0,
+                 "learned": 53.0, "mixed_cold": 57.0, "fp64_cold": 93.0, "e2e": 54.0, "cpu_sample": 15.0}
+
 
 def metric_for(args):
     return f"LPs/sec to {args.eps:g} rel KKT"
@@ -69,12 +75,17 @@ def parse():
     ap.add_argument("--batch-count", type=int, default=4096, help="instances of the batched workloads")
     ap.add_argument("--eps", type=float, default=None,
                     help="relative KKT tolerance (default 1e-8 for ill_conditioned, else 1e-6)")
+    ap.add_argument("--eps-objective", type=float, default=1e-6,
+                    help="an answer also needs its objective within this relative distance of the optimum (FP64 "
+                         "bound on the device); 0 = relative KKT alone")
+    ap.add_argument("--compare-steps", type=int, default=1,
+                    help="refinery_learned: steps of each comparison leg (cold mixed, cold FP64)")
     ap.add_argument("--no-fp64", action="store_true", help="skip the plain FP64 comparison leg")
     ap.add_argument("--time-limit", type=float, default=None,
                     help="single-LP workloads: seconds per solve before it stops as INTERRUPTED "
                          "(default 1200 for ill_conditioned, else none)")
     ap.add_argument("--e2e-steps", type=int, default=None,
-                    help="single-LP workloads: end-to-end steps (default = --steps; 0 skips the e2e leg)")
+                    help="end-to-end steps (default 1 for refinery_learned, else = --steps; 0 skips the e2e leg)")
     ap.add_argument("--cpu-sample-iters", type=int, default=20)
     ap.add_argument("--profile-scale", type=float, default=1.0,
                     help="--profile with ill_conditioned: rows and columns scaled by this factor (0.4 keeps each "
@@ -90,7 +101,7 @@ def parse():
     if a.time_limit is None:
         a.time_limit = 1200.0 if a.workload == "ill_conditioned" else 0.0
     if a.e2e_steps is None:
-        a.e2e_steps = a.steps
+        a.e2e_steps = 1 if a.workload == "refinery_learned" else a.steps
     return a
 
 
@@ -436,10 +447,13 @@ def learned_cfg(args, fam, world):
     return {"workload": "refinery_planning_learned_warm_start", "m": fam.m, "n": fam.n, "nnz": int(fam.rowptr[-1]),
             "params": fam.N_PARAM, "train_instances": args.train_count, "label_eps": args.label_eps,
             "heldout_instances": args.heldout, "mlp": f"{fam.N_PARAM}->1024->1024->{fam.n + fam.m + 1} GELU bf16/fp32acc",
-            "epochs": args.epochs, "eps_rel_kkt": args.eps, "shared_matrix": True, "family_seed": 3,
+            "epochs": args.epochs, "eps_rel_kkt": args.eps, "eps_objective": args.eps_objective,
+            "shared_matrix": True, "family_seed": 3,
             "heldout_seed": 20001, "parallelism": f"replicas x{world}",
             "l2": "per-instance vectors of 2000 instances (~300 MB) exceed L2; the shared matrix is L2-resident",
-            "warmup": "warm-up steps run the same solves capped at 2048 iterations (autotuning, graphs, allocations)"}
+            "warmup": "warm-up steps run the same solves capped at 2048 iterations (autotuning, graphs, allocations)",
+            "steps": {"learned (value)": args.steps, "mixed_cold": args.compare_steps, "fp64_cold": args.compare_steps,
+                      "e2e": args.e2e_steps}}
 
 
 def timed_leg(ctx, torch, world, steps, fn):
@@ -457,24 +471,45 @@ def timed_leg(ctx, torch, world, steps, fn):
     return max_over_ranks(e0.elapsed_time(e1), world), out
 
 
+def planned_wall_s(args):
+    """Planned wall time (s) of the refinery_learned run from its leg counts and the
+    per-leg times measured on one B200 (LEARNED_LEG_S): untimed labels and training,
+    warm-up solves, the value leg x --steps, the comparison legs x --compare-steps,
+    the e2e leg x --e2e-steps and the CPU sample."""
+    t = LEARNED_LEG_S
+    scale = args.heldout / 2000.0
+    return (t["start"] + t["label_per_instance"] * args.train_count + t["epoch"] * args.epochs
+            + args.warmup * t["warmup_step"]
+            + scale * (args.steps * t["learned"] + args.compare_steps * (t["mixed_cold"] + t["fp64_cold"])
+                       + args.e2e_steps * t["e2e"])
+            + t["cpu_sample"])
+
+
 def run_learned_workload(args):
     import torch
+    t_wall0 = time.perf_counter()
     rank, world, local = dist_setup(args.gpus)
     torch.cuda.set_device(local)
     torch.cuda.set_stream(torch.cuda.Stream())  # CUDA graphs need a non-default stream
     b2p, fam, P = learned_setup(args, rank)
     ctx = b2p.Context(local)
     ctx.set_stream(torch.cuda.current_stream().cuda_stream)
+    plan = planned_wall_s(args)
+    if rank == 0:
+        print(f"[bench] planned wall time {plan:.0f} s", file=sys.stderr, flush=True)
     ws = b2p.warmstart.LearnedWarmStart(ctx, fam)
     fit = ws.fit(n_train=args.train_count, label_eps=args.label_eps, epochs=args.epochs)
     s0 = b2p.warmstart.upload_family(ctx, fam, P)
     F = P.astype(np.float32)
-    common = dict(eps=args.eps, max_iterations=400000)
+    # every leg stops on the same judge: relative KKT <= eps and the answer's objective
+    # within eps_objective of the optimum (FP64 bound evaluated on the device)
+    judge = dict(eps=args.eps, eps_objective=args.eps_objective)
+    cap = 400000
     legs = {
-        "learned": lambda it: ctx.batch_solve_learned(F, fallback=True, precision="fp32", eps=args.eps,
-                                                      max_iterations=it, outputs=False),
-        "mixed_cold": lambda it: ctx.batch_solve(precision="fp32", eps=args.eps, max_iterations=it, outputs=False),
-        "fp64_cold": lambda it: ctx.batch_solve(precision="fp64", eps=args.eps, max_iterations=it, outputs=False),
+        "learned": lambda it: ctx.batch_solve_learned(F, fallback=True, precision="fp32", max_iterations=it,
+                                                      outputs=False, **judge),
+        "mixed_cold": lambda it: ctx.batch_solve(precision="fp32", max_iterations=it, outputs=False, **judge),
+        "fp64_cold": lambda it: ctx.batch_solve(precision="fp64", max_iterations=it, outputs=False, **judge),
     }
     for _ in range(args.warmup):
         for fn in legs.values():
@@ -486,23 +521,31 @@ def run_learned_workload(args):
         pass
     res = {}
     clocks = None
+    steps_of = {"learned": args.steps, "mixed_cold": args.compare_steps, "fp64_cold": args.compare_steps}
     for name, fn in legs.items():
+        k = steps_of[name]
+        if k <= 0:
+            continue
         sampler = ClockSampler(uuid) if name == "learned" else None
         if sampler:
             sampler.start()
-        ms, (summ, per, _, _) = timed_leg(ctx, torch, world, args.steps, lambda: fn(common["max_iterations"]))
+        ms, (summ, per, _, _) = timed_leg(ctx, torch, world, k, lambda: fn(cap))
         if sampler:
             clocks = sampler.stop()
-        solved = sum_over_ranks(float((per["status"] == 0).sum()), world)
-        res[name] = {"value": solved * args.steps / (ms / 1e3), "unit": "LPs/s", "ms_per_step": ms / args.steps,
+        objs = ctx.batch_objectives()
+        ok = per["status"] == 0
+        solved = sum_over_ranks(float(ok.sum()), world)
+        res[name] = {"value": solved * k / (ms / 1e3), "unit": "LPs/s", "steps": k, "ms_per_step": ms / k,
                      "solved": int(solved), "instances": args.heldout * world,
                      "iterations_mean": float(per["iterations"].mean()),
                      "iterations_max": int(per["iterations"].max()), "worst_rel_kkt": float(per["rel_kkt"].max()),
+                     "worst_obj_err_solved": float(objs["obj_err"][ok].max()) if ok.any() else None,
+                     "statuses": {str(v): int((per["status"] == v).sum()) for v in np.unique(per["status"])},
                      "kernel_ms": summ["kernel_time_ms"], "kernel_launches": summ["kernel_launches"]}
         if name == "learned":
             res[name]["fallbacks"] = summ["fallbacks"]
             res[name]["warm_used"] = int(per["warm_used"].sum())
-            launches = int(summ["kernel_launches"]) * args.steps
+            launches = int(summ["kernel_launches"]) * k
             it_total = float(per["iterations"].sum())
             kern_ms = summ["kernel_time_ms"]
     # end to end through the public API: pinned host parameter vectors and instance
@@ -517,54 +560,79 @@ def run_learned_workload(args):
     def e2e_step():
         ctx.batch_upload([(s0.m, s0.n, s0.rowptr, s0.colidx, s0.vals)], np.zeros(args.heldout, np.int32),
                          pin["b"].numpy(), pin["c"].numpy(), pin["lb"].numpy(), pin["ub"].numpy(), pin["is_eq"].numpy())
-        return ctx.batch_solve_learned(pin["f"].numpy(), fallback=True, precision="fp32", **common)
+        return ctx.batch_solve_learned(pin["f"].numpy(), fallback=True, precision="fp32", max_iterations=cap, **judge)
 
-    e2e_ms, (esumm, eper, ex, ey) = timed_leg(ctx, torch, world, args.steps, e2e_step)
-    esolved = sum_over_ranks(float((eper["status"] == 0).sum()), world)
-    e2e = {"value": esolved * args.steps / (e2e_ms / 1e3), "unit": "LPs/s", "h2d_bytes_per_step": h2d,
-           "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms / args.steps,
-           "note": "batch upload (host CSR checks, renumbering, device transpose, scaling) + learned solve + x, y"}
-    # roofline of the dominant kernel (k_batch_chunk, FP32): algorithmic bytes of every
-    # instance-iteration of the learned leg over its kernel time
+    e2e = {"value": None, "skipped": "--e2e-steps 0", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h}
+    if args.e2e_steps > 0:
+        e2e_ms, (esumm, eper, ex, ey) = timed_leg(ctx, torch, world, args.e2e_steps, e2e_step)
+        esolved = sum_over_ranks(float((eper["status"] == 0).sum()), world)
+        e2e = {"value": esolved * args.e2e_steps / (e2e_ms / 1e3), "unit": "LPs/s", "h2d_bytes_per_step": h2d,
+               "d2h_bytes_per_step": d2h, "steps": args.e2e_steps, "ms_per_step": e2e_ms / args.e2e_steps,
+               "solved": int(esolved),
+               "note": "batch upload (host CSR checks, renumbering, device transpose, scaling) + learned solve + x, y"}
+    # roofline of the dominant kernel (k_batch_chunk<float>): algorithmic bytes of every
+    # instance-iteration of the value leg over its kernel time.  The shared matrix and the
+    # instances' vectors are served from L2 and shared memory, so the bound that applies is
+    # the on-chip one; the DRAM share comes from the committed ncu capture.
     nnz = int(fam.rowptr[-1])
     per_iter = 12 * nnz + 24 * fam.n + 16 * fam.m
     peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
     peak = peaks.get("hbm_gbs", 6650.0)
     achieved = it_total * per_iter / (kern_ms / 1e3) / 1e9
-    traffic = None  # ncu dram read + write of one k_batch_chunk launch / its instance-iterations
-    tfile = ROOT / "profiles" / "batch_chunk_refinery_planning.txt"
-    if tfile.exists():
-        for ln in tfile.read_text().splitlines():
-            if ln.startswith("dram_bytes_per_instance_iteration:"):
-                traffic = float(ln.split(":")[1])
-    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "traffic": traffic, "traffic_unit": "DRAM bytes per instance-iteration (ncu)",
-                "kernel": "k_batch_chunk<float> (SELL-32, learned leg)",
+    prof = read_profile(ROOT / "profiles" / "batch_chunk_refinery_planning.txt")
+    roofline = {"bound": "l2", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": prof.get("dram_bytes_per_instance_iteration"),
+                "traffic_unit": "DRAM bytes per instance-iteration (ncu dram__bytes_read.sum + write.sum)",
+                "dram_frac": (prof["dram_bytes_per_instance_iteration"] / per_iter
+                              if "dram_bytes_per_instance_iteration" in prof else None),
+                "l2_bytes_per_instance_iteration": prof.get("l2_bytes_per_instance_iteration"),
+                "lts_throughput_pct": prof.get("lts_throughput_pct"),
+                "kernel": "k_batch_chunk<float> (SELL, learned leg)",
                 "algorithmic_bytes_per_instance_iteration": per_iter,
-                "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if peaks else "fallback 6650 (of fallback)",
+                "peak_source": ("MEASURED_PEAKS.json hbm_gbs (of measured); no measured L2 peak exists, so the "
+                                "fraction is against HBM" if peaks else "fallback 6650 (of fallback)"),
                 "note": "12 B per nonzero (FP32 value + 16-bit index, both orientations), 24 B per column, 16 B per "
-                        "row; the shared matrix is served from L2, so DRAM traffic is far below these bytes"}
+                        "row; bound 'l2': the shared matrix and the instances' vectors stay in L2 / shared memory "
+                        "(ncu: DRAM carries dram_frac of these bytes)"}
     cpu = None
     if rank == 0 and world == 1:
         lp0 = fam.instance(P[0])
         # ~10 s of one host core: 120k reference iterations on a held-out instance
-        cpu = cpu_reference_sample(lp0, 120000, int(res["fp64_cold"]["iterations_mean"]))
+        cpu = cpu_reference_sample(lp0, 120000, int(res["fp64_cold"]["iterations_mean"])
+                                   if "fp64_cold" in res else HALPERN_ITERS["refinery_learned"])
     if rank == 0:
-        ratio = res["learned"]["value"] / res["fp64_cold"]["value"]
+        ratio = (res["learned"]["value"] / res["fp64_cold"]["value"]) if "fp64_cold" in res else None
         line = {"metric": METRIC_LEARNED, "value": res["learned"]["value"], "unit": "LPs/s", "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": res["learned"]["ms_per_step"],
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
                 "dtype": "f32 (SpMV, vectors) + f64 (scaling, KKT, re-centring); bf16 MLP",
                 "data": "synthetic (seeded refinery planning family, no dataset)",
                 "config": learned_cfg(args, fam, world), "learned_vs_fp64_cold": ratio,
-                "learned": res["learned"], "mixed_cold": res["mixed_cold"], "fp64_cold": res["fp64_cold"],
+                "judge": {"eps_rel_kkt": args.eps, "eps_objective": args.eps_objective,
+                          "counted": "status OPTIMAL: FP64 relative KKT <= eps on the original instance and the "
+                                     "FP64 objective-error bound <= eps_objective, both on the device"},
+                "learned": res["learned"], "mixed_cold": res.get("mixed_cold"), "fp64_cold": res.get("fp64_cold"),
                 "training": fit, "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "gpu_launches": launches,
-                "clocks": clocks}
+                "clocks": clocks, "wall_s": time.perf_counter() - t_wall0, "planned_wall_s": plan}
         print(json.dumps(line), flush=True)
     ctx.close()
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
+
+
+def read_profile(path):
+    """`name: value` lines of a committed ncu summary (numbers only)."""
+    out = {}
+    if path.exists():
+        for ln in path.read_text().splitlines():
+            if ":" in ln:
+                k, v = ln.split(":", 1)
+                try:
+                    out[k.strip()] = float(v.split()[0])
+                except (ValueError, IndexError):
+                    pass
+    return out
 
 
 def _ref_worker(q):

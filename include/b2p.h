@@ -119,6 +119,21 @@ typedef struct {
                                        CSR kernel with that many lanes per row; -1 = SELL kernel, 32-row
                                        slices; -2 = the same with gather windows in shared memory;
                                        -3 / -4 = SELL kernel, 16- / 8-row slices (2 / 4 lanes per row) */
+    /* Halpern and batched engines */
+    double  eps_objective;          /* 0 = off (default).  > 0: OPTIMAL also needs the answer's objective
+                                       c.x within eps_objective * max(1, |c.x|) of the optimum, judged by
+                                       the FP64 bound max(c.x - d(y), sum_i |y_i| viol_i(x)): d(y) is the
+                                       dual objective (a lower bound on the optimum when the reduced costs
+                                       are absorbed by the bounds), the sum bounds how far below the
+                                       optimum an infeasible x can reach to first order */
+    double  eps_infeasible;         /* 1e-8: PDLP-style certificates from the fixed-point displacement
+                                       T(z) - z at every check.  Dual ray dy (primal infeasible): its ray
+                                       objective -b.dy + sum_j min(a_j l_j, a_j u_j), a = A^T dy, is > 0
+                                       and the violations of a on unbounded sides are <= eps_infeasible
+                                       times it -> B2P_STATUS_INFEASIBLE_DETECTED.  Primal ray dx (dual
+                                       infeasible): c.dx < 0 and the violations of A dx and of the bound
+                                       recession cone are <= eps_infeasible |c.dx| ->
+                                       B2P_STATUS_UNBOUNDED_DETECTED.  0 = off */
 } b2p_params;
 
 typedef struct {
@@ -186,7 +201,10 @@ int b2p_norm2(void* ctx, size_t n, const double* a, double* out, b2p_timing_t* t
  *     that first call before any stream capture on that device.
  *   - Every call shares the array (each call overwrites all it reads), so two
  *     calls that can run at the same time on the GPU -- on different streams or
- *     from different threads -- race; serialise them on one stream. */
+ *     from different threads -- race; serialise them on one stream.
+ *   - A CUDA error left pending by earlier work is returned as this call's
+ *     status and nothing is launched.  The set-up is cached per device for the
+ *     life of the process: cudaDeviceReset is not supported. */
 #define B2P_TOO_LARGE           8
 #define B2P_DOT_NOALLOC_MAX_N   8388608
 int b2p_dot_noalloc(const double* a_dev, const double* b_dev, size_t n, double* out_dev, void* stream);
@@ -230,6 +248,14 @@ int b2p_batch_upload(void* ctx, int nmat, const int32_t* mat_m, const int32_t* m
 int b2p_batch_solve(void* ctx, const b2p_params* params, const double* x0, const double* y0, const double* omega0,
                     int32_t* status_out, int64_t* iters_out, double* kkt_out, double* omega_out, double* x_out,
                     double* y_out, b2p_result* summary);
+
+/* Per-instance objectives of the last batched solve (count each; any pointer may
+ * be null): the primal objective c.x, the dual objective d(y) -- a valid lower
+ * bound on the optimum when every column is boxed, which is what a
+ * branch-and-bound search prunes on (the reference prunes on the node LP's
+ * objective, src/branch_and_bound.cpp:517-537) -- and the FP64 bound on the
+ * relative objective error of the answer (see b2p_params.eps_objective). */
+int b2p_batch_objectives(void* ctx, double* pobj_out, double* dobj_out, double* obj_err_out);
 
 /* ---- learned warm start: MLP in -> h -> h -> out, GELU, BF16 weights and
  *      activations, FP32 accumulation on the tcgen05 tensor cores ---- */

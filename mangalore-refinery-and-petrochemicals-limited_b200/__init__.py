@@ -49,7 +49,7 @@ class Params(C.Structure):
                 ("reflection", C.c_double), ("restart_sufficient", C.c_double), ("restart_necessary", C.c_double),
                 ("restart_artificial", C.c_double), ("primal_weight", C.c_double), ("step_safety", C.c_double),
                 ("refinement_rounds", C.c_int), ("time_limit_s", C.c_double),
-                ("lanes_per_row", C.c_int)]
+                ("lanes_per_row", C.c_int), ("eps_objective", C.c_double), ("eps_infeasible", C.c_double)]
 
 
 class Result(C.Structure):
@@ -93,6 +93,7 @@ SIGNATURES = {
     "b2p_batch_upload": (C.c_int, [_P, C.c_int, _I32P, _I32P, _I64P, _I32P, _I32P, _F64P, C.c_int, _I32P, _F64P,
                                    _F64P, _F64P, _F64P, _U8P]),
     "b2p_batch_solve": (C.c_int, [_P, C.POINTER(Params), _P, _P, _P, _P, _P, _P, _P, _P, _P, C.POINTER(Result)]),
+    "b2p_batch_objectives": (C.c_int, [_P, _P, _P, _P]),
     "b2p_mlp_create": (C.c_int, [_P, C.c_int, C.c_int, C.c_int, C.c_uint64]),
     "b2p_mlp_train_epoch": (C.c_int, [_P, _F32P, _F32P, C.c_int, C.c_int, C.c_float, C.POINTER(C.c_float)]),
     "b2p_mlp_infer": (C.c_int, [_P, _F32P, C.c_int, _F32P]),
@@ -300,6 +301,14 @@ class Context:
         self._check(lib().b2p_batch_solve(self._h, C.byref(p), _ptr(x0), _ptr(y0), _ptr(om), _ptr(st), _ptr(it),
                                           _ptr(kk), _ptr(omo), _ptr(x), _ptr(y), C.byref(r)))
         return _result_dict(r), {"status": st, "iterations": it, "rel_kkt": kk, "omega": omo}, x, y
+
+    def batch_objectives(self):
+        """Per-instance primal objective c.x, dual objective d(y) and FP64 bound on the
+        relative objective error of the last batched solve (b2p_batch_objectives)."""
+        cnt = len(self.batch_m)
+        p, d, e = np.zeros(cnt), np.zeros(cnt), np.zeros(cnt)
+        self._check(lib().b2p_batch_objectives(self._h, _ptr(p), _ptr(d), _ptr(e)))
+        return {"pobj": p, "dobj": d, "obj_err": e}
 
     def batch_solve_learned(self, features, fallback=True, outputs=True, **params):
         """Learned warm start for every instance of the uploaded batch (see

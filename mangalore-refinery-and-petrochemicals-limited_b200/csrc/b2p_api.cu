@@ -233,6 +233,8 @@ void b2p_params_default(b2p_params* p) {
     p->refinement_rounds = -1;
     p->time_limit_s = 0.0;
     p->lanes_per_row = 0;
+    p->eps_objective = 0.0;
+    p->eps_infeasible = 1e-8;
 }
 
 int b2p_device_info(int device, b2p_device_info_t* out) {

@@ -67,6 +67,7 @@ namespace b2p {
 struct InstCtrl {
     double omega, r0, rprev;
     double rel_p, rel_d, rel_g, pobj, dobj;
+    double obj_err;  // FP64 bound on |c.x - optimum| / max(1, |c.x|) at the last check
     long long k, total, restarts;
     long long base;  // iterations spent on the instance before this run (cold fallback after a warm run)
     int status, done, first;
@@ -96,8 +97,9 @@ struct BatchWork {
     DBuf<int64_t> x_off, y_off;
     DBuf<double> b, c, lb, ub, bnorm, cnorm;
     DBuf<uint8_t> is_eq;
-    // packed records and iterates, sized for FP64 and reinterpreted for FP32
-    DBuf<double> colp, rowp, x, xt, y, yt;
+    // packed records and iterates, sized for FP64 and reinterpreted for FP32; dx, dy hold
+    // the fixed-point displacement T(z) - z of the last check (infeasibility certificates)
+    DBuf<double> colp, rowp, x, xt, y, yt, dx, dy;
     bool recenter = false;
     DBuf<double> xbar, atybar, ybar, axbar;  // re-centring state (per instance, original space)
     DBuf<InstCtrl> ictrl;
@@ -153,11 +155,13 @@ struct BArgs {
     double *bnorm, *cnorm;  // written by the init kernel
     const uint8_t* is_eq;
     void *colp, *rowp, *x, *xt, *y, *yt;  // MT-typed
+    void *dx, *dy;                        // MT-typed: T(z) - z at check iterations (eps_inf > 0)
     InstCtrl* ictrl;
     const int32_t* active;
     int32_t* counters;
     // parameters
     double eps, beta_s, beta_n, beta_a, rho;
+    double eps_obj, eps_inf;  // objective-accuracy stop (0 = off), certificate tolerance (0 = off)
     // FP64 re-centring: per-instance centre in the original space, A xbar, A^T ybar;
     // original FP64 values in both orientations
     int recenter;
@@ -170,7 +174,7 @@ struct BArgs {
 template <typename T>
 __device__ __forceinline__ T clampT(T v, T lo, T hi) { return v < lo ? lo : (v > hi ? hi : v); }
 
-// Block-wide FP64 sum of up to 6 values, fixed reduction order (deterministic).
+// Block-wide FP64 sum of NV values (sh holds 32 * NV), fixed reduction order (deterministic).
 template <int NV>
 __device__ __forceinline__ void block_sums(double (&v)[NV], double* sh /* [32*NV] */) {
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
@@ -257,14 +261,188 @@ __device__ void rebuild_shifted(const BArgs& a, int m, int n, int64_t ro, int64_
     }
 }
 
+// Restart-check iteration of one instance, run by every thread of the owning CTA
+// after T(z) (xt, yt) and, with certificates on, the displacement (dx, dy) are in
+// global memory: the FP64 KKT of T(z) on the original instance, the objective-error
+// bound, the certificates (every fourth check) and the decisions -- termination,
+// restart, primal weight -- which thread 0 writes to `sc` and `s_flags` (0: done,
+// 1: restart).  Kept out of line: its FP64 accumulators would otherwise raise the
+// register demand of the iteration loop.
+template <typename MT>
+__device__ __noinline__ void check_instance(const BArgs& a, int inst, int m, int n, int64_t ro, int64_t co,
+                                            int64_t xo, int64_t yo, long long total, long long kk, double om,
+                                            double r_now, double dxa, double dya, InstCtrl& sc, int* s_flags,
+                                            double* red) {
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
+    const int csub = lane & (kKktLanesCol - 1), cgid = warp * (32 / kKktLanesCol) + lane / kKktLanesCol;
+    const int cgroups = nwarps * (32 / kKktLanesCol);
+    const int rsub = lane & (kKktLanesRow - 1), rgid = warp * (32 / kKktLanesRow) + lane / kKktLanesRow;
+    const int rgroups = nwarps * (32 / kKktLanesRow);
+    const MT *xtg = (const MT*)a.xt, *ytg = (const MT*)a.yt;
+    const MT *dxg = (const MT*)a.dx, *dyg = (const MT*)a.dy;
+    const bool rays = a.eps_inf > 0.0;
+    // ---- FP64 KKT of T(z) on the original instance (CSR, sub-warp per row / column) and the
+    // objective-error bound
+    double kk2[6] = {0, 0, 0, 0, 0, 0};
+    // |primal residual|^2, b.y, |dual residual|^2, c.x, bound term, sum |y| viol
+    for (int base = 0; base < m; base += rgroups) {
+        const int i = base + rgid;
+        double s = 0.0;
+        if (i < m) {
+            const int64_t gi = ro + i;
+            for (int e = a.rowptr[gi] + rsub; e < a.rowptr[gi + 1]; e += kKktLanesRow)
+                s += a.sv64[e] * (double)xtg[xo + a.colidx[e] - co];
+        }
+#pragma unroll
+        for (int o = kKktLanesRow / 2; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if (i < m && rsub == 0) {
+            const double dri = a.dr[ro + i];
+            const double ax = (a.recenter ? a.axbar[yo + i] : 0.0) + s / dri;
+            double rp = ax - a.b[yo + i];
+            if (!a.is_eq[yo + i]) rp = fmax(rp, 0.0);
+            kk2[0] += rp * rp;
+            const double yv = (a.recenter ? a.ybar[yo + i] : 0.0) + dri * (double)ytg[yo + i];
+            kk2[1] += a.b[yo + i] * yv;
+            kk2[5] += fabs(yv) * fabs(rp);
+        }
+    }
+    for (int base = 0; base < n; base += cgroups) {
+        const int j = base + cgid;
+        double s = 0.0;
+        if (j < n) {
+            const int64_t gj = co + j;
+            for (int e = a.t_rowptr[gj] + csub; e < a.t_rowptr[gj + 1]; e += kKktLanesCol)
+                s += a.stv64[e] * (double)ytg[yo + a.t_colidx[e] - ro];
+        }
+#pragma unroll
+        for (int o = kKktLanesCol / 2; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if (j < n && csub == 0) {
+            const double dcj = a.dc[co + j];
+            const double cj = a.c[xo + j], lj = a.lb[xo + j], uj = a.ub[xo + j];
+            const double g = cj + (a.recenter ? a.atybar[xo + j] : 0.0) + s / dcj;
+            const bool fl = isfinite(lj), fu = isfinite(uj);
+            const double lam = (fl && fu) ? g : (fl ? fmax(g, 0.0) : (fu ? fmin(g, 0.0) : 0.0));
+            const double rd = g - lam;
+            kk2[2] += rd * rd;
+            kk2[3] += cj * ((a.recenter ? a.xbar[xo + j] : 0.0) + dcj * (double)xtg[xo + j]);
+            if (lam > 0.0) kk2[4] += lam * lj;
+            else if (lam < 0.0) kk2[4] += lam * uj;
+        }
+    }
+    block_sums<6>(kk2, red);
+    // ---- certificates of the displacement dx, dy = T(z) - z (every fourth check): primal
+    // ray dx -- 0 |viol of A dx and of the bounds' recession cone|^2, 1 c.dx, 2 sum |c dx|;
+    // dual ray dy -- 3 b.dy, 4 bound term of a = A^T dy, 5 sum of |terms|, 6 |viol of a|^2
+    double ry[7] = {0, 0, 0, 0, 0, 0, 0};
+    const bool ray_check = rays && ((total / a.K) & 3) == 0;
+    if (ray_check) {
+        for (int base = 0; base < m; base += rgroups) {
+            const int i = base + rgid;
+            double s = 0.0;
+            if (i < m) {
+                const int64_t gi = ro + i;
+                for (int e = a.rowptr[gi] + rsub; e < a.rowptr[gi + 1]; e += kKktLanesRow)
+                    s += a.sv64[e] * (double)dxg[xo + a.colidx[e] - co];
+            }
+#pragma unroll
+            for (int o = kKktLanesRow / 2; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+            if (i < m && rsub == 0) {
+                const double dri = a.dr[ro + i];
+                const double adx = s / dri;  // (A dx)_i in the original space
+                const double v = a.is_eq[yo + i] ? adx : fmax(adx, 0.0);
+                ry[0] += v * v;
+                const double dyo = dri * (double)dyg[yo + i];
+                ry[3] += a.b[yo + i] * dyo;
+                ry[5] += fabs(a.b[yo + i] * dyo);
+            }
+        }
+        for (int base = 0; base < n; base += cgroups) {
+            const int j = base + cgid;
+            double s = 0.0;
+            if (j < n) {
+                const int64_t gj = co + j;
+                for (int e = a.t_rowptr[gj] + csub; e < a.t_rowptr[gj + 1]; e += kKktLanesCol)
+                    s += a.stv64[e] * (double)dyg[yo + a.t_colidx[e] - ro];
+            }
+#pragma unroll
+            for (int o = kKktLanesCol / 2; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+            if (j < n && csub == 0) {
+                const double dcj = a.dc[co + j];
+                const double cj = a.c[xo + j], lj = a.lb[xo + j], uj = a.ub[xo + j];
+                const bool fl = isfinite(lj), fu = isfinite(uj);
+                const double dxo = dcj * (double)dxg[xo + j];
+                ry[1] += cj * dxo;
+                ry[2] += fabs(cj * dxo);
+                const double bv = (fl && dxo < 0.0 ? -dxo : 0.0) + (fu && dxo > 0.0 ? dxo : 0.0);
+                ry[0] += bv * bv;
+                const double at = s / dcj;  // (A^T dy)_j in the original space
+                const double t = at > 0.0 ? (fl ? at * lj : 0.0) : (at < 0.0 ? (fu ? at * uj : 0.0) : 0.0);
+                ry[4] += t;
+                ry[5] += fabs(t);
+                const double av = (!fl && at > 0.0 ? at : 0.0) + (!fu && at < 0.0 ? -at : 0.0);
+                ry[6] += av * av;
+            }
+        }
+        block_sums<7>(ry, red);
+    }
+    if (tid == 0) {
+        const double pres = sqrt(kk2[0]), dres = sqrt(kk2[2]);
+        const double pobj = kk2[3], dobj = -kk2[1] + kk2[4];
+        sc.rel_p = pres / (1.0 + a.bnorm[inst]);
+        sc.rel_d = dres / (1.0 + a.cnorm[inst]);
+        sc.rel_g = fabs(pobj - dobj) / (1.0 + fabs(pobj) + fabs(dobj));
+        sc.pobj = pobj;
+        sc.dobj = dobj;
+        sc.obj_err = fmax(fmax(pobj - dobj, kk2[5]), 0.0) / fmax(1.0, fabs(pobj));
+        const bool finite = isfinite(pres) && isfinite(dres) && isfinite(pobj) && isfinite(dobj) && isfinite(r_now);
+        const bool obj_ok = a.eps_obj <= 0.0 || sc.obj_err <= a.eps_obj;
+        // certificates (ratio tests of PDLP; the 1e-9 floors keep rounding noise of a
+        // vanishing displacement from passing for a ray)
+        const double dray = -ry[3] + ry[4], pray = ry[1];
+        const bool infeas = ray_check && dray > 0.0 && dray > 1e-9 * ry[5] && sqrt(ry[6]) <= a.eps_inf * dray;
+        const bool unbnd = ray_check && pray < 0.0 && -pray > 1e-9 * ry[2] && sqrt(ry[0]) <= a.eps_inf * -pray;
+        if (!finite) {
+            sc.done = 1;
+            sc.status = B2P_STATUS_NUMERICAL_FAILURE;
+        } else if (sc.rel_p <= a.eps && sc.rel_d <= a.eps && sc.rel_g <= a.eps && obj_ok) {
+            sc.done = 1;
+            sc.status = B2P_STATUS_OPTIMAL;
+        } else if (infeas) {
+            sc.done = 1;
+            sc.status = B2P_STATUS_INFEASIBLE_DETECTED;
+        } else if (unbnd) {
+            sc.done = 1;
+            sc.status = B2P_STATUS_UNBOUNDED_DETECTED;
+        } else if (total + sc.base >= a.max_iter) {
+            sc.done = 1;
+            sc.status = B2P_STATUS_MAX_ITERATIONS;
+        }
+        s_flags[1] = 0;
+        if (!sc.done) {
+            const bool rs = (r_now <= a.beta_s * sc.r0) || (r_now <= a.beta_n * sc.r0 && r_now > sc.rprev) ||
+                            ((double)kk >= a.beta_a * (double)total);
+            sc.rprev = r_now;
+            if (rs) {
+                if (dxa > 1e-10 && dya > 1e-10) {
+                    const double nw = exp(0.5 * log(dya / dxa) + 0.5 * log(om));
+                    if (isfinite(nw) && nw > 0.0) sc.omega = nw;
+                }
+                sc.restarts += 1;
+                s_flags[1] = 1;
+            }
+        }
+        s_flags[0] = sc.done;
+    }
+}
+
 // Body of the persistent chunk kernel; launched as k_batch_chunk (the tuned CTA
 // size, up to 512 threads, two CTAs per SM) while many instances are active and as
 // k_batch_chunk_wide (1024 threads, one CTA per SM) once no more than one instance
 // per SM is left, so the last, slowest instances iterate with twice the threads.
 template <typename MT>
-__device__ __forceinline__ void batch_chunk_body(BArgs a, int chunk) {
+__device__ __forceinline__ void batch_chunk_body(const BArgs& a, int chunk) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    __shared__ double red[32 * 6];
+    __shared__ double red[32 * 7];
     __shared__ InstCtrl sc;
     __shared__ int s_q;
     __shared__ int s_flags[2];  // 0: done, 1: restart
@@ -277,11 +455,9 @@ __device__ __forceinline__ void batch_chunk_body(BArgs a, int chunk) {
     ColP<MT>* colp = (ColP<MT>*)a.colp;
     RowP<MT>* rowp = (RowP<MT>*)a.rowp;
     MT *xg = (MT*)a.x, *xtg = (MT*)a.xt, *yg = (MT*)a.y, *ytg = (MT*)a.yt;
+    MT *dxg = (MT*)a.dx, *dyg = (MT*)a.dy;
+    const bool rays = a.eps_inf > 0.0;
     const int active_count = a.counters[1];
-    const int csub = lane & (kKktLanesCol - 1), cgid = warp * (32 / kKktLanesCol) + lane / kKktLanesCol;
-    const int cgroups = nwarps * (32 / kKktLanesCol);
-    const int rsub = lane & (kKktLanesRow - 1), rgid = warp * (32 / kKktLanesRow) + lane / kKktLanesRow;
-    const int rgroups = nwarps * (32 / kKktLanesRow);
     const MT rho = (MT)a.rho, one_rho = (MT)(1.0 + a.rho);
     while (true) {
         if (tid == 0) s_q = atomicAdd(&a.counters[0], 1);
@@ -339,6 +515,7 @@ __device__ __forceinline__ void batch_chunk_body(BArgs a, int chunk) {
                     }
                     if (check) {
                         xtg[xo + j] = xt;
+                        if (rays) dxg[xo + j] = xt - x0;
                         const double e = (double)xt - (double)p.a;
                         acc[1] += e * e;
                     }
@@ -368,6 +545,11 @@ __device__ __forceinline__ void batch_chunk_body(BArgs a, int chunk) {
                     }
                     if (check) {
                         ytg[yo + i] = yt;
+                        if (rays) {  // a dual ray candidate keeps y >= 0 on <= rows (p.lo = -inf on = rows)
+                            MT d = yt - y0;
+                            if (p.lo != (MT)(-INFINITY) && d < (MT)0) d = (MT)0;
+                            dyg[yo + i] = d;
+                        }
                         const double e = (double)yt - (double)p.a;
                         acc[3] += e * e;
                     }
@@ -401,86 +583,7 @@ __device__ __forceinline__ void batch_chunk_body(BArgs a, int chunk) {
                 dya = sqrt(acc[3]);
             }
             __syncthreads();  // xt / yt of this iteration are in global memory
-            // ---- FP64 KKT of T(z) on the original instance (CSR, sub-warp per row / column)
-            double kk2[6] = {0, 0, 0, 0, 0, 0};  // |primal residual|^2, b.y, |dual residual|^2, c.x, bound term
-            for (int base = 0; base < m; base += rgroups) {
-                const int i = base + rgid;
-                double s = 0.0;
-                if (i < m) {
-                    const int64_t gi = ro + i;
-                    for (int e = a.rowptr[gi] + rsub; e < a.rowptr[gi + 1]; e += kKktLanesRow)
-                        s += a.sv64[e] * (double)xtg[xo + a.colidx[e] - co];
-                }
-#pragma unroll
-                for (int o = kKktLanesRow / 2; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-                if (i < m && rsub == 0) {
-                    const double dri = a.dr[ro + i];
-                    const double ax = (a.recenter ? a.axbar[yo + i] : 0.0) + s / dri;
-                    double rp = ax - a.b[yo + i];
-                    if (!a.is_eq[yo + i]) rp = fmax(rp, 0.0);
-                    kk2[0] += rp * rp;
-                    kk2[1] += a.b[yo + i] * ((a.recenter ? a.ybar[yo + i] : 0.0) + dri * (double)ytg[yo + i]);
-                }
-            }
-            for (int base = 0; base < n; base += cgroups) {
-                const int j = base + cgid;
-                double s = 0.0;
-                if (j < n) {
-                    const int64_t gj = co + j;
-                    for (int e = a.t_rowptr[gj] + csub; e < a.t_rowptr[gj + 1]; e += kKktLanesCol)
-                        s += a.stv64[e] * (double)ytg[yo + a.t_colidx[e] - ro];
-                }
-#pragma unroll
-                for (int o = kKktLanesCol / 2; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-                if (j < n && csub == 0) {
-                    const double dcj = a.dc[co + j];
-                    const double cj = a.c[xo + j], lj = a.lb[xo + j], uj = a.ub[xo + j];
-                    const double g = cj + (a.recenter ? a.atybar[xo + j] : 0.0) + s / dcj;
-                    const bool fl = isfinite(lj), fu = isfinite(uj);
-                    const double lam = (fl && fu) ? g : (fl ? fmax(g, 0.0) : (fu ? fmin(g, 0.0) : 0.0));
-                    const double rd = g - lam;
-                    kk2[2] += rd * rd;
-                    kk2[3] += cj * ((a.recenter ? a.xbar[xo + j] : 0.0) + dcj * (double)xtg[xo + j]);
-                    if (lam > 0.0) kk2[4] += lam * lj;
-                    else if (lam < 0.0) kk2[4] += lam * uj;
-                }
-            }
-            block_sums<6>(kk2, red);
-            if (tid == 0) {
-                const double pres = sqrt(kk2[0]), dres = sqrt(kk2[2]);
-                const double pobj = kk2[3], dobj = -kk2[1] + kk2[4];
-                sc.rel_p = pres / (1.0 + a.bnorm[inst]);
-                sc.rel_d = dres / (1.0 + a.cnorm[inst]);
-                sc.rel_g = fabs(pobj - dobj) / (1.0 + fabs(pobj) + fabs(dobj));
-                sc.pobj = pobj;
-                sc.dobj = dobj;
-                const bool finite = isfinite(pres) && isfinite(dres) && isfinite(pobj) && isfinite(dobj) && isfinite(r_now);
-                if (!finite) {
-                    sc.done = 1;
-                    sc.status = B2P_STATUS_NUMERICAL_FAILURE;
-                } else if (sc.rel_p <= a.eps && sc.rel_d <= a.eps && sc.rel_g <= a.eps) {
-                    sc.done = 1;
-                    sc.status = B2P_STATUS_OPTIMAL;
-                } else if (total + sc.base >= a.max_iter) {
-                    sc.done = 1;
-                    sc.status = B2P_STATUS_MAX_ITERATIONS;
-                }
-                s_flags[1] = 0;
-                if (!sc.done) {
-                    const bool rs = (r_now <= a.beta_s * sc.r0) || (r_now <= a.beta_n * sc.r0 && r_now > sc.rprev) ||
-                                    ((double)kk >= a.beta_a * (double)total);
-                    sc.rprev = r_now;
-                    if (rs) {
-                        if (dxa > 1e-10 && dya > 1e-10) {
-                            const double nw = exp(0.5 * log(dya / dxa) + 0.5 * log(om));
-                            if (isfinite(nw) && nw > 0.0) sc.omega = nw;
-                        }
-                        sc.restarts += 1;
-                        s_flags[1] = 1;
-                    }
-                }
-                s_flags[0] = sc.done;
-            }
+            check_instance<MT>(a, inst, m, n, ro, co, xo, yo, total, kk, om, r_now, dxa, dya, sc, s_flags, red);
             __syncthreads();
             done = s_flags[0] != 0;
             om = sc.omega;
@@ -528,12 +631,12 @@ __device__ __forceinline__ void batch_chunk_body(BArgs a, int chunk) {
 }
 
 template <typename MT>
-__global__ void __launch_bounds__(512, 2) k_batch_chunk(BArgs a, int chunk) {
+__global__ void __launch_bounds__(512, 2) k_batch_chunk(const __grid_constant__ BArgs a, int chunk) {
     batch_chunk_body<MT>(a, chunk);
 }
 
 template <typename MT>
-__global__ void __launch_bounds__(1024, 1) k_batch_chunk_wide(BArgs a, int chunk) {
+__global__ void __launch_bounds__(1024, 1) k_batch_chunk_wide(const __grid_constant__ BArgs a, int chunk) {
     batch_chunk_body<MT>(a, chunk);
 }
 
@@ -961,6 +1064,8 @@ BArgs make_args(BatchWork* w, const b2p_params* p, const int32_t* active) {
     a.xt = w->xt.p;
     a.y = w->y.p;
     a.yt = w->yt.p;
+    a.dx = w->dx.p;
+    a.dy = w->dy.p;
     a.ictrl = w->ictrl.p;
     a.active = active;
     a.counters = w->counters.p;
@@ -969,6 +1074,8 @@ BArgs make_args(BatchWork* w, const b2p_params* p, const int32_t* active) {
     a.beta_n = p->restart_necessary;
     a.beta_a = p->restart_artificial;
     a.rho = p->reflection;
+    a.eps_obj = p->eps_objective;
+    a.eps_inf = (w->dx.p && w->dy.p) ? p->eps_infeasible : 0.0;
     a.max_iter = p->max_iterations;
     a.K = p->check_every;
     a.recenter = w->recenter ? 1 : 0;
@@ -1016,6 +1123,7 @@ int autotune(Ctx* ctx, BatchWork* w, const b2p_params* p, TuneCfg* best) {
     b2p_params tp = *p;
     tp.max_iterations = 1LL << 40;
     tp.eps_rel_kkt = 0.0;  // never terminates inside the trial
+    tp.eps_infeasible = 0.0;
     const int trial_iters = 128;
     float best_ms = 1e30f;
     *best = {256, 2048};
@@ -1083,6 +1191,11 @@ int batch_run(Ctx* ctx, BatchWork* w, const b2p_params* p, const double* x0_dev,
         if (st) return st;
         w->tuned_threads[prec] = cfg.threads;
     }
+    // displacement buffers of the infeasibility certificates (sized for FP64, read as MT)
+    if (p->eps_infeasible > 0.0) {
+        B2P_CUDA(ctx, w->dx.reserve(IN));
+        B2P_CUDA(ctx, w->dy.reserve(IM));
+    }
     // re-centring: on by default for the mixed engine (refinement_rounds < 0), forced by > 0
     w->recenter = p->refinement_rounds > 0 || (p->refinement_rounds < 0 && sizeof(MT) == 4);
     if (w->recenter) {
@@ -1144,9 +1257,24 @@ int batch_run(Ctx* ctx, BatchWork* w, const b2p_params* p, const double* x0_dev,
     const bool have_wide = per_sm_w >= 1;
     const int grid_w = ctx->sm_count * std::max(per_sm_w, 1);
     // one graph = two chunk launches with compaction (ping-pong active lists); a second
-    // graph does the same with the wide kernel
-    cudaGraph_t graph = nullptr, graph_w = nullptr;
-    cudaGraphExec_t exec = nullptr, exec_w = nullptr;
+    // graph does the same with the wide kernel.  The guard releases the graphs, their
+    // executables and the pinned counter copy on every way out of this function.
+    struct Owned {
+        cudaGraph_t graph[2] = {nullptr, nullptr};
+        cudaGraphExec_t exec[2] = {nullptr, nullptr};
+        int32_t* host_cnt = nullptr;
+        ~Owned() {
+            for (int g = 0; g < 2; ++g) {
+                if (exec[g]) cudaGraphExecDestroy(exec[g]);
+                if (graph[g]) cudaGraphDestroy(graph[g]);
+            }
+            if (host_cnt) cudaFreeHost(host_cnt);
+        }
+    } own;
+    cudaGraph_t& graph = own.graph[0];
+    cudaGraph_t& graph_w = own.graph[1];
+    cudaGraphExec_t& exec = own.exec[0];
+    cudaGraphExec_t& exec_w = own.exec[1];
     for (int g = 0; g < (have_wide ? 2 : 1); ++g) {
         B2P_CUDA(ctx, cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
         if (g == 0) fn<<<grid, cfg.threads, sm, s>>>(a1, cfg.chunk);
@@ -1159,17 +1287,18 @@ int batch_run(Ctx* ctx, BatchWork* w, const b2p_params* p, const double* x0_dev,
         cudaGraphExec_t& ex = g == 0 ? exec : exec_w;
         cudaError_t ce = cudaStreamEndCapture(s, &gr);
         if (ce != cudaSuccess) {
+            gr = nullptr;
             ctx->err = std::string("batch graph capture: ") + cudaGetErrorString(ce);
             return B2P_EXECUTION_FAILED;
         }
         ce = cudaGraphInstantiate(&ex, gr, 0);
         if (ce != cudaSuccess) {
-            cudaGraphDestroy(gr);
+            ex = nullptr;
             ctx->err = std::string("batch graph instantiate: ") + cudaGetErrorString(ce);
             return B2P_EXECUTION_FAILED;
         }
     }
-    int32_t* host_cnt = nullptr;
+    int32_t*& host_cnt = own.host_cnt;
     B2P_CUDA(ctx, cudaMallocHost(&host_cnt, 2 * sizeof(int32_t)));
     const int64_t max_graphs = p->max_iterations / (2LL * cfg.chunk) + 3;
     int64_t graphs = 0;
@@ -1192,13 +1321,6 @@ int batch_run(Ctx* ctx, BatchWork* w, const b2p_params* p, const double* x0_dev,
     }
     cudaEventRecord(ctx->ev1, s);
     B2P_CUDA(ctx, cudaStreamSynchronize(s));
-    cudaFreeHost(host_cnt);
-    cudaGraphExecDestroy(exec);
-    cudaGraphDestroy(graph);
-    if (have_wide) {
-        cudaGraphExecDestroy(exec_w);
-        cudaGraphDestroy(graph_w);
-    }
     ctx->launches += graphs * 4;
     float kms = 0;
     cudaEventElapsedTime(&kms, ctx->ev0, ctx->ev1);
@@ -1585,6 +1707,22 @@ int b2p_batch_solve(void* p, const b2p_params* params, const double* x0, const d
     return B2P_OK;
 }
 
+int b2p_batch_objectives(void* p, double* pobj_out, double* dobj_out, double* obj_err_out) {
+    Ctx* ctx = static_cast<Ctx*>(p);
+    if (!ctx) return B2P_GPU_UNINITIALIZED;
+    BatchWork* w = ctx->bw;
+    if (!w || !w->solved || (int)w->hc.size() != w->count) {
+        ctx->err = "b2p_batch_objectives: no batched solve to report";
+        return B2P_NO_LP;
+    }
+    for (int i = 0; i < w->count; ++i) {
+        if (pobj_out) pobj_out[i] = w->hc[i].pobj;
+        if (dobj_out) dobj_out[i] = w->hc[i].dobj;
+        if (obj_err_out) obj_err_out[i] = w->hc[i].obj_err;
+    }
+    return B2P_OK;
+}
+
 int b2p_batch_solve_learned(void* p, const b2p_params* params, const float* features, int fallback,
                             int32_t* status_out, int64_t* iters_out, double* kkt_out, uint8_t* warm_used_out,
                             double* x_out, double* y_out, b2p_result* summary) {
@@ -1639,7 +1777,11 @@ int b2p_batch_solve_learned(void* p, const b2p_params* params, const float* feat
     std::vector<int32_t> failed;
     for (int i = 0; i < w->count; ++i) {
         warm_iters[i] = w->hc[i].total;
-        const bool ok = w->hc[i].done && w->hc[i].status == B2P_STATUS_OPTIMAL;
+        // an answer, or a certificate of infeasibility / unboundedness (which holds
+        // whatever the starting point), ends the instance
+        const int sti = w->hc[i].status;
+        const bool ok = w->hc[i].done && (sti == B2P_STATUS_OPTIMAL || sti == B2P_STATUS_INFEASIBLE_DETECTED ||
+                                          sti == B2P_STATUS_UNBOUNDED_DETECTED);
         if (!ok && warm_iters[i] < pp->max_iterations) failed.push_back(i);
     }
     if (fallback && !failed.empty() && !timed_out) {

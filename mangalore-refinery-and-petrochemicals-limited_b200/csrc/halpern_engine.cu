@@ -54,6 +54,9 @@ namespace b2p {
 enum {
     A_RX2 = 0, A_RY2, A_RX2_FIRST, A_RY2_FIRST, A_DXA2, A_DYA2,   // restart residuals
     A_PRES2, A_DRES2, A_PC, A_BY, A_LAM,                          // KKT pieces
+    A_EST,                                                        // sum |y| viol (objective-error bound)
+    A_PRV2, A_PRC, A_PRM,           // primal ray dx: |viol|^2, c.dx, sum |c dx|
+    A_DRB, A_DRL, A_DRM, A_DRV2,    // dual ray dy: b.dy, bound term of A^T dy, sum |terms|, |viol|^2
     A_COUNT
 };
 
@@ -61,8 +64,9 @@ struct Ctrl {
     double acc[A_COUNT];
     double omega, eta, tau, sigma;
     double r0, rprev;
-    double rel_p, rel_d, rel_g, pobj, dobj;
+    double rel_p, rel_d, rel_g, pobj, dobj, obj_err;
     double eps, beta_s, beta_n, beta_a, bnorm, cnorm;
+    double eps_obj, eps_inf;  // objective-accuracy stop, certificate tolerance (0 = off)
     // refinement: the solved (correction) problem maps back to the original LP as
     // x = xbar + pscale * dc * xt, y = ybar + dscale * dr * yt; the solve also stops
     // (status kInnerDone) once its fixed-point residual fell to inner_tol * r_first
@@ -127,6 +131,8 @@ struct HalpernWork {
     DBuf<float> sv32, stv32;       // scaled A and A^T, FP32 (FP32 engine)
     DBuf<double> c64, b64, l64, u64;
     DBuf<double> x, xa, xt, y, ya, yt;  // FP64 iterates (both precisions)
+    DBuf<double> xd, yd;                 // T(z) - z of the last check (infeasibility certificates)
+    bool rays = false;                   // certificates on for the current solve
     DBuf<double> xh64;                   // gathered operand, FP64 engine
     DBuf<float> xh32, yg32;              // gathered operands, mixed engine
     // FP64 re-centring: current centre in the original space, A xbar, A^T ybar, shifted dual bound
@@ -315,6 +321,7 @@ struct IterArgs {
     VT* zh;                // primal: xh out (dual: unused)
     const double* za;      // anchor
     double* zt;            // T(z) at check iterations
+    double* zd;            // T(z) - z at check iterations (null = certificates off); dual: >= 0 on <= rows
     Ctrl* ctrl;
     int rows;
     double rho;
@@ -493,6 +500,7 @@ __global__ void __launch_bounds__(1024) k_iter(IterArgs<VT, GT> a, int it) {
             }
             if (MODE == M_CHECK) {
                 a.zt[row] = zt;
+                if (a.zd) a.zd[row] = (!PRIMAL && lo[u] != -INFINITY) ? fmax(zt - zr[u], 0.0) : zt - zr[u];
                 const double e = zt - za;
                 acc_d += e * e;
             }
@@ -643,6 +651,7 @@ __global__ void __launch_bounds__(1024) k_iter_sell(IterArgs<VT, GT> a, int it) 
         }
         if (MODE == M_CHECK) {
             a.zt[row] = zt;
+            if (a.zd) a.zd[row] = (!PRIMAL && lo != -INFINITY) ? fmax(zt - zr, 0.0) : zt - zr;
             const double e = zt - zan;
             acc_d += e * e;
         }
@@ -794,57 +803,95 @@ struct KktMap {
     const double* atybar; // n: A^T ybar
 };
 
+// rows: primal residual, b.y, the objective-error sum |y| viol; with xd / yd (the
+// displacement T(z) - z), A xd for the primal ray and the row terms of the dual ray
 template <int L>
 __global__ void __launch_bounds__(TB) k_kkt_rows(int m, const int32_t* __restrict__ ptr, const int32_t* __restrict__ idx,
                                                  const double* __restrict__ v64, const double* __restrict__ xt,
                                                  const double* __restrict__ yt, const double* __restrict__ b,
                                                  const uint8_t* __restrict__ is_eq, const double* __restrict__ dr,
-                                                 KktMap map, Ctrl* ctrl) {
+                                                 KktMap map, const double* __restrict__ xd,
+                                                 const double* __restrict__ yd, Ctrl* ctrl) {
     if (ctrl->done) return;
     const double ps = ctrl->pscale, ds = ctrl->dscale;
     const int lane = threadIdx.x & 31, sub = lane & (L - 1), rpw = 32 / L;
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
-    double p2 = 0.0, by = 0.0;
+    const bool rays = xd != nullptr;
+    double p2 = 0.0, by = 0.0, est = 0.0, prv = 0.0, drb = 0.0, drm = 0.0;
     for (int base = warp * rpw; base < m; base += nw * rpw) {
         int r = base + lane / L;
         bool valid = r < m;
-        double s = 0.0;
+        double s = 0.0, sd = 0.0;
         if (valid)
-            for (int k = ptr[r] + sub; k < ptr[r + 1]; k += L) s += v64[k] * xt[idx[k]];
+            for (int k = ptr[r] + sub; k < ptr[r + 1]; k += L) {
+                s += v64[k] * xt[idx[k]];
+                if (rays) sd += v64[k] * xd[idx[k]];
+            }
 #pragma unroll
-        for (int o = L / 2; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        for (int o = L / 2; o > 0; o >>= 1) {
+            s += __shfl_xor_sync(0xffffffffu, s, o);
+            sd += __shfl_xor_sync(0xffffffffu, sd, o);
+        }
         if (valid && sub == 0) {
+            const bool eq = is_eq[r] != 0;
             double ax = (map.axbar ? map.axbar[r] : 0.0) + ps * (s / dr[r]);
             double rp = ax - b[r];
-            if (!is_eq[r]) rp = fmax(rp, 0.0);
+            if (!eq) rp = fmax(rp, 0.0);
             p2 += rp * rp;
-            by += b[r] * ((map.ybar ? map.ybar[r] : 0.0) + ds * (dr[r] * yt[r]));
+            const double yv = (map.ybar ? map.ybar[r] : 0.0) + ds * (dr[r] * yt[r]);
+            by += b[r] * yv;
+            est += fabs(yv) * fabs(rp);
+            if (rays) {
+                const double adx = sd / dr[r];  // (A dx)_r, original space
+                const double v = eq ? adx : fmax(adx, 0.0);
+                prv += v * v;
+                const double dyo = dr[r] * yd[r];
+                drb += b[r] * dyo;
+                drm += fabs(b[r] * dyo);
+            }
         }
     }
     block_sum_to(p2, &ctrl->acc[A_PRES2]);
     block_sum_to(by, &ctrl->acc[A_BY]);
+    block_sum_to(est, &ctrl->acc[A_EST]);
+    if (rays) {
+        block_sum_to(prv, &ctrl->acc[A_PRV2]);
+        block_sum_to(drb, &ctrl->acc[A_DRB]);
+        block_sum_to(drm, &ctrl->acc[A_DRM]);
+    }
 }
 
 // columns: reduced cost g = c + A^T y, bound multipliers lambda, dual residual, c.x and the bound terms
+// columns: reduced cost g = c + A^T y, bound multipliers lambda, dual residual, c.x and the bound
+// terms; with xd / yd, the column terms of the primal ray and A^T yd for the dual ray
 template <int L>
 __global__ void __launch_bounds__(TB) k_kkt_cols(int n, const int32_t* __restrict__ ptr, const int32_t* __restrict__ idx,
                                                  const double* __restrict__ v64, const double* __restrict__ yt,
                                                  const double* __restrict__ xt, const double* __restrict__ c,
                                                  const double* __restrict__ lb, const double* __restrict__ ub,
-                                                 const double* __restrict__ dc, KktMap map, Ctrl* ctrl) {
+                                                 const double* __restrict__ dc, KktMap map,
+                                                 const double* __restrict__ xd, const double* __restrict__ yd,
+                                                 Ctrl* ctrl) {
     if (ctrl->done) return;
     const double ps = ctrl->pscale, ds = ctrl->dscale;
     const int lane = threadIdx.x & 31, sub = lane & (L - 1), rpw = 32 / L;
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
-    double d2 = 0.0, pc = 0.0, lam_t = 0.0;
+    const bool rays = yd != nullptr;
+    double d2 = 0.0, pc = 0.0, lam_t = 0.0, prv = 0.0, prc = 0.0, prm = 0.0, drl = 0.0, drm = 0.0, drv = 0.0;
     for (int base = warp * rpw; base < n; base += nw * rpw) {
         int j = base + lane / L;
         bool valid = j < n;
-        double s = 0.0;
+        double s = 0.0, sd = 0.0;
         if (valid)
-            for (int k = ptr[j] + sub; k < ptr[j + 1]; k += L) s += v64[k] * yt[idx[k]];
+            for (int k = ptr[j] + sub; k < ptr[j + 1]; k += L) {
+                s += v64[k] * yt[idx[k]];
+                if (rays) sd += v64[k] * yd[idx[k]];
+            }
 #pragma unroll
-        for (int o = L / 2; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        for (int o = L / 2; o > 0; o >>= 1) {
+            s += __shfl_xor_sync(0xffffffffu, s, o);
+            sd += __shfl_xor_sync(0xffffffffu, sd, o);
+        }
         if (valid && sub == 0) {
             double g = c[j] + (map.atybar ? map.atybar[j] : 0.0) + ds * (s / dc[j]);
             bool fl = isfinite(lb[j]), fu = isfinite(ub[j]);
@@ -855,11 +902,32 @@ __global__ void __launch_bounds__(TB) k_kkt_cols(int n, const int32_t* __restric
             pc += c[j] * x;
             if (lam > 0.0) lam_t += lam * lb[j];
             else if (lam < 0.0) lam_t += lam * ub[j];
+            if (rays) {
+                const double dxo = dc[j] * xd[j];
+                prc += c[j] * dxo;
+                prm += fabs(c[j] * dxo);
+                const double bv = (fl && dxo < 0.0 ? -dxo : 0.0) + (fu && dxo > 0.0 ? dxo : 0.0);
+                prv += bv * bv;
+                const double at = sd / dc[j];  // (A^T dy)_j, original space
+                const double t = at > 0.0 ? (fl ? at * lb[j] : 0.0) : (at < 0.0 ? (fu ? at * ub[j] : 0.0) : 0.0);
+                drl += t;
+                drm += fabs(t);
+                const double av = (!fl && at > 0.0 ? at : 0.0) + (!fu && at < 0.0 ? -at : 0.0);
+                drv += av * av;
+            }
         }
     }
     block_sum_to(d2, &ctrl->acc[A_DRES2]);
     block_sum_to(pc, &ctrl->acc[A_PC]);
     block_sum_to(lam_t, &ctrl->acc[A_LAM]);
+    if (rays) {
+        block_sum_to(prv, &ctrl->acc[A_PRV2]);
+        block_sum_to(prc, &ctrl->acc[A_PRC]);
+        block_sum_to(prm, &ctrl->acc[A_PRM]);
+        block_sum_to(drl, &ctrl->acc[A_DRL]);
+        block_sum_to(drm, &ctrl->acc[A_DRM]);
+        block_sum_to(drv, &ctrl->acc[A_DRV2]);
+    }
 }
 
 // One thread: termination, restart and primal-weight decisions for the chunk just run.
@@ -881,13 +949,27 @@ __global__ void k_control(Ctrl* c) {
     c->rel_g = fabs(pobj - dobj) / (1.0 + fabs(pobj) + fabs(dobj));
     c->pobj = pobj;
     c->dobj = dobj;
+    c->obj_err = fmax(fmax(pobj - dobj, a[A_EST]), 0.0) / fmax(1.0, fabs(pobj));
     bool finite = isfinite(pres) && isfinite(dres) && isfinite(pobj) && isfinite(dobj) && isfinite(r);
+    const bool obj_ok = c->eps_obj <= 0.0 || c->obj_err <= c->eps_obj;
+    // PDLP's ratio tests on the rays; the 1e-9 floors keep the rounding noise of a
+    // vanishing displacement from passing for a ray
+    const bool rays = c->eps_inf > 0.0;
+    const double dray = -a[A_DRB] + a[A_DRL], pray = a[A_PRC];
+    const bool infeas = rays && dray > 0.0 && dray > 1e-9 * a[A_DRM] && sqrt(a[A_DRV2]) <= c->eps_inf * dray;
+    const bool unbnd = rays && pray < 0.0 && -pray > 1e-9 * a[A_PRM] && sqrt(a[A_PRV2]) <= c->eps_inf * -pray;
     if (!finite) {
         c->done = 1;
         c->status = B2P_STATUS_NUMERICAL_FAILURE;
-    } else if (c->rel_p <= c->eps && c->rel_d <= c->eps && c->rel_g <= c->eps) {
+    } else if (c->rel_p <= c->eps && c->rel_d <= c->eps && c->rel_g <= c->eps && obj_ok) {
         c->done = 1;
         c->status = B2P_STATUS_OPTIMAL;
+    } else if (infeas && c->inner_tol <= 0.0) {
+        c->done = 1;
+        c->status = B2P_STATUS_INFEASIBLE_DETECTED;
+    } else if (unbnd && c->inner_tol <= 0.0) {
+        c->done = 1;
+        c->status = B2P_STATUS_UNBOUNDED_DETECTED;
     } else if (c->total >= c->max_iter) {
         c->done = 1;
         c->status = B2P_STATUS_MAX_ITERATIONS;
@@ -1030,8 +1112,10 @@ void launch_iter(int mode, int L, int R, unsigned grid, int tb, cudaStream_t s, 
 
 void launch_kkt(int Lr, int Lc, unsigned gr, unsigned gc, cudaStream_t s, const DevLP& lp, HalpernWork* w,
                 const KktMap& map, Ctrl* ctrl) {
-#define KR(LL) k_kkt_rows<LL><<<gr, TB, 0, s>>>(lp.m, lp.rowptr.p, lp.colidx.p, w->sv64.p, w->xt.p, w->yt.p, lp.b.p, lp.is_eq.p, w->dr.p, map, ctrl)
-#define KC(LL) k_kkt_cols<LL><<<gc, TB, 0, s>>>(lp.n, lp.t_rowptr.p, lp.t_colidx.p, w->stv64.p, w->yt.p, w->xt.p, lp.c.p, lp.lb.p, lp.ub.p, w->dc.p, map, ctrl)
+    const double* xd = w->rays ? w->xd.p : nullptr;
+    const double* yd = w->rays ? w->yd.p : nullptr;
+#define KR(LL) k_kkt_rows<LL><<<gr, TB, 0, s>>>(lp.m, lp.rowptr.p, lp.colidx.p, w->sv64.p, w->xt.p, w->yt.p, lp.b.p, lp.is_eq.p, w->dr.p, map, xd, yd, ctrl)
+#define KC(LL) k_kkt_cols<LL><<<gc, TB, 0, s>>>(lp.n, lp.t_rowptr.p, lp.t_colidx.p, w->stv64.p, w->yt.p, w->xt.p, lp.c.p, lp.lb.p, lp.ub.p, w->dc.p, map, xd, yd, ctrl)
     switch (Lr) { case 1: KR(1); break; case 2: KR(2); break; case 4: KR(4); break; case 8: KR(8); break; case 16: KR(16); break; default: KR(32); }
     switch (Lc) { case 1: KC(1); break; case 2: KC(2); break; case 4: KC(4); break; case 8: KC(8); break; case 16: KC(16); break; default: KC(32); }
 #undef KR
@@ -1317,8 +1401,8 @@ struct Ops<float> {
 template <typename MT>
 IterArgs<MT, double> primal_args(const DevLP& L, HalpernWork* w, const b2p_params* p, bool sell) {
     IterArgs<MT, double> a{L.t_rowptr.p, L.t_colidx.p, Ops<MT>::stv(w), w->y.p, w->c64.p, w->l64.p, w->u64.p,
-                           nullptr, nullptr, w->x.p, Ops<MT>::xh(w), w->xa.p, w->xt.p, w->ctrl.p, L.n,
-                           p->reflection, nullptr};
+                           nullptr, nullptr, w->x.p, Ops<MT>::xh(w), w->xa.p, w->xt.p,
+                           w->rays ? w->xd.p : nullptr, w->ctrl.p, L.n, p->reflection, nullptr};
     if (sell) {
         a.ptr = nullptr;
         a.idx = w->sc->idx.p;
@@ -1332,8 +1416,8 @@ IterArgs<MT, double> primal_args(const DevLP& L, HalpernWork* w, const b2p_param
 template <typename MT>
 IterArgs<MT, MT> dual_args(const DevLP& L, HalpernWork* w, const b2p_params* p, bool sell) {
     IterArgs<MT, MT> a{L.rowptr.p, L.colidx.p, Ops<MT>::sv(w), Ops<MT>::xh(w), w->b64.p, nullptr, nullptr, L.is_eq.p,
-                       w->recenter ? w->ylb_s.p : nullptr, w->y.p, nullptr, w->ya.p, w->yt.p, w->ctrl.p, L.m,
-                       p->reflection, nullptr};
+                       w->recenter ? w->ylb_s.p : nullptr, w->y.p, nullptr, w->ya.p, w->yt.p,
+                       w->rays ? w->yd.p : nullptr, w->ctrl.p, L.m, p->reflection, nullptr};
     if (sell) {
         a.ptr = nullptr;
         a.idx = w->sr->idx.p;
@@ -1728,6 +1812,11 @@ int solve_T(Ctx* ctx, HalpernWork* w, const b2p_params* p, const double* x0, con
             B2P_CUDA(ctx, cudaMemsetAsync(b->p, 0, sizeof(double) * m, s));
         }
     }
+    w->rays = p->eps_infeasible > 0.0;
+    if (w->rays) {
+        B2P_CUDA(ctx, w->xd.reserve(n));
+        B2P_CUDA(ctx, w->yd.reserve(m));
+    }
     int st = prepare_scaling(ctx, w, p->ruiz_iterations, mixed);
     if (st) return st;
     // SELL layouts: the 32-row one always, the others once the tuner has built them;
@@ -1799,6 +1888,8 @@ int solve_T(Ctx* ctx, HalpernWork* w, const b2p_params* p, const double* x0, con
     hc.tau = eta / omega;
     hc.sigma = eta * omega;
     hc.eps = p->eps_rel_kkt;
+    hc.eps_obj = p->eps_objective;
+    hc.eps_inf = w->rays ? p->eps_infeasible : 0.0;
     hc.beta_s = p->restart_sufficient;
     hc.beta_n = p->restart_necessary;
     hc.beta_a = p->restart_artificial;

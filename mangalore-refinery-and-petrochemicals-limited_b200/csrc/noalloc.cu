@@ -70,7 +70,11 @@ __global__ void __launch_bounds__(kNaThreads) k_na_sum(int count, const double* 
     }
 }
 
-// Set-up for the current device: resolve the scratch array's device address once.
+// Set-up for the current device: resolve the scratch array's device address once,
+// and load both kernels onto the device (with lazy module loading a kernel is
+// otherwise loaded at its first launch, which could then fall inside a later stream
+// capture -- a first call with n == 0 never launches k_na_partials).  The cache is
+// per device ordinal and is not invalidated: cudaDeviceReset is not supported.
 int scratch_for_current_device(double** out) {
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return B2P_GPU_UNAVAILABLE;
@@ -79,6 +83,10 @@ int scratch_for_current_device(double** out) {
         void* ptr = nullptr;
         cudaError_t e = cudaGetSymbolAddress(&ptr, g_dot_scratch);
         if (e != cudaSuccess || !ptr) return map_cuda_error(e == cudaSuccess ? cudaErrorInvalidSymbol : e);
+        cudaFuncAttributes fa;
+        e = cudaFuncGetAttributes(&fa, k_na_partials);
+        if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, k_na_sum);
+        if (e != cudaSuccess) return map_cuda_error(e);
         g_scratch_addr[dev] = static_cast<double*>(ptr);
     }
     *out = g_scratch_addr[dev];
@@ -95,6 +103,10 @@ extern "C" int b2p_dot_noalloc(const double* a_dev, const double* b_dev, size_t 
     double* scratch = nullptr;
     int st = scratch_for_current_device(&scratch);
     if (st != B2P_OK) return st;
+    // an error left pending by earlier, unrelated work is reported (not cleared) and
+    // nothing is launched, so the status after the launches is this call's own
+    cudaError_t pre = cudaPeekAtLastError();
+    if (pre != cudaSuccess) return map_cuda_error(pre);
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     const int blocks = n == 0 ? 0 : (int)((n + (size_t)kNaThreads * kNaItems - 1) / ((size_t)kNaThreads * kNaItems));
     if (blocks > 0) k_na_partials<<<blocks, kNaThreads, 0, s>>>(n, a_dev, b_dev, scratch);

@@ -216,6 +216,14 @@ FirstOrderSolverResult GPUFirstOrderSolver::solve(const LPModel& model) {
             result.status = FirstOrderSolverStatus::INTERRUPTED;
             result.message = "B200 first-order engine stopped at its time limit.";
             break;
+        case B2P_STATUS_INFEASIBLE_DETECTED:
+            result.status = FirstOrderSolverStatus::INFEASIBLE_DETECTED;
+            result.message = "B200 first-order engine found a dual ray certifying primal infeasibility.";
+            break;
+        case B2P_STATUS_UNBOUNDED_DETECTED:
+            result.status = FirstOrderSolverStatus::UNBOUNDED_DETECTED;
+            result.message = "B200 first-order engine found a primal ray certifying unboundedness.";
+            break;
         default:
             result.status = FirstOrderSolverStatus::NUMERICAL_FAILURE;
             result.message = "B200 first-order engine reported a numerical failure.";

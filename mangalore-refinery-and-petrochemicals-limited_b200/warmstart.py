@@ -61,10 +61,14 @@ class LearnedWarmStart:
         return self.stats
 
     def solve(self, P, eps: float = 1e-6, fallback: bool = True, precision: str = "fp32",
-              max_iterations: int = 1_000_000, outputs: bool = True, upload: bool = True):
+              max_iterations: int = 1_000_000, outputs: bool = True, upload: bool = True,
+              eps_objective: float = 0.0):
         """Learned-warm batched solve of the instances of P (uploads them unless
-        upload=False, when they are already the context's batch)."""
+        upload=False, when they are already the context's batch).  eps_objective > 0
+        also asks each answer's objective to be within that relative distance of the
+        optimum (b2p_params.eps_objective)."""
         if upload:
             upload_family(self.ctx, self.family, P)
         return self.ctx.batch_solve_learned(np.asarray(P, np.float32), fallback=fallback, precision=precision,
-                                            eps=eps, max_iterations=max_iterations, outputs=outputs)
+                                            eps=eps, eps_objective=eps_objective, max_iterations=max_iterations,
+                                            outputs=outputs)

@@ -145,3 +145,53 @@ def test_batch_instance_too_large_is_an_error(ctx, lpgen, b2p):
         ctx.batch_solve(precision="fp32", eps=1e-6, max_iterations=1000, outputs=False)
     assert e.value.code == b2p.INVALID_ARGUMENT
     assert "shared memory" in str(e.value)
+
+
+def _planning_judge(per, x, y, fam, P, s0, B, Cc, LB, UB, EQ, lpgen, reflib, zs, eps):
+    """Every answer: FP64 relative KKT <= eps (oracle), objective within eps of the
+    HiGHS optimum with the max(1, |z|) denominator of the reference's
+    docs/testing-strategy.md:56, and the reference SolutionVerifier accepts x at
+    the absolute feasibility tolerance eps (1 + ||b||) that a relative primal
+    residual of eps allows."""
+    assert np.all(per["status"] == 0), (per["status"], per["iterations"])
+    for i in range(len(P)):
+        s = lpgen.StdLP(s0.m, s0.n, s0.rowptr, s0.colidx, s0.vals, B[i], Cc[i], LB[i], UB[i], EQ[i])
+        xi, yi = x[i * fam.n:(i + 1) * fam.n], y[i * fam.m:(i + 1) * fam.m]
+        k = pdlp_oracle.kkt(s, xi, yi)
+        assert k["rel_kkt"] <= 1.05 * eps, (i, k)
+        assert abs(k["pobj"] - zs[i]) <= eps * max(1.0, abs(zs[i])), (i, k["pobj"], zs[i])
+        lp = fam.instance(P[i])
+        v = reflib.verify(lp, xi, feas_tol=eps * (1 + float(np.linalg.norm(B[i]))), reported_obj=float(lp.obj @ xi))
+        assert v["verified"] == 1, (i, v)
+
+
+def test_planning_heldout_judge_cold(ctx, lpgen, b2p, reflib):
+    """The benchmark's stop criterion (relative KKT 1e-6 and the device's objective-error
+    bound 1e-6) on its first 64 held-out instances, mixed precision from the cold
+    start: every answer passes the north-star judge."""
+    import json
+    from conftest import GOLDEN
+    g = json.loads((GOLDEN / "planning_heldout_highs.json").read_text())
+    fam = lpgen.RefineryPlanningFamily()
+    P = fam.sample_params(g["count"], g["seed"])
+    s0, B, Cc, LB, UB, EQ = fam.standard_batch(P)
+    b2p.warmstart.upload_family(ctx, fam, P)
+    _, per, x, y = ctx.batch_solve(precision="fp32", eps=1e-6, eps_objective=1e-6, max_iterations=400000)
+    objs = ctx.batch_objectives()
+    assert np.all(objs["obj_err"] <= 1e-6)
+    _planning_judge(per, x, y, fam, P, s0, B, Cc, LB, UB, EQ, lpgen, reflib, g["objectives"], 1e-6)
+
+
+def test_planning_heldout_judge_learned(ctx, lpgen, b2p, reflib):
+    """The same 64 instances learned-warm (a small model: 512 labels to 1e-8, 30 epochs)
+    at the benchmark's stop criterion: every warm-started answer passes the judge."""
+    import json
+    from conftest import GOLDEN
+    g = json.loads((GOLDEN / "planning_heldout_highs.json").read_text())
+    fam = lpgen.RefineryPlanningFamily()
+    ws = b2p.warmstart.LearnedWarmStart(ctx, fam)
+    ws.fit(n_train=512, label_eps=1e-8, epochs=30, max_iterations=400000)
+    P = fam.sample_params(g["count"], g["seed"])
+    s0, B, Cc, LB, UB, EQ = fam.standard_batch(P)
+    summ, per, x, y = ws.solve(P, eps=1e-6, eps_objective=1e-6, max_iterations=400000)
+    _planning_judge(per, x, y, fam, P, s0, B, Cc, LB, UB, EQ, lpgen, reflib, g["objectives"], 1e-6)

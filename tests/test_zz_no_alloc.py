@@ -37,8 +37,11 @@ def test_dot_noalloc_matches_dot_twice(b2p):
             b_dev = torch.from_numpy(b).cuda()
             out_dev = torch.full((1,), np.nan, dtype=torch.float64, device="cuda")
             torch.cuda.synchronize()
+            free_before = torch.cuda.mem_get_info()[0]
             assert _noalloc_dot(b2p, torch, a_dev, b_dev, out_dev, n, stream) == b2p.OK
             stream.synchronize()
+            if n != 1_000_003:  # after the first call (its set-up) no device memory moves
+                assert torch.cuda.mem_get_info()[0] == free_before
             got = float(out_dev.item())
             # same two-pass FP64 algorithm, different block partition: agree to rounding
             assert abs(got - want) <= 1e-12 * float(np.abs(a) @ np.abs(b)), (n, got, want)
