@@ -222,6 +222,33 @@ int b2p_upload_lp(void* ctx, int m, int n, int64_t nnz, const int32_t* rowptr, c
 int b2p_solve(void* ctx, const b2p_params* params, const double* x0, const double* y0, b2p_result* result,
               double* x_out, double* y_out);
 
+/* ---- MPS -> device ingest (replaces MpsParser::parse_file,
+ *      include/bharatopt/mps_parser.hpp:40-48, src/mps_parser.cpp:140-531, on the way
+ *      to the engine).  The file is read on the host in one pass straight into CSR, with
+ *      the reference parser's semantics (sections, markers, first RHS / RANGES / BOUNDS
+ *      vector, range table, bound types, objective offset); b2p_upload_mps uploads its
+ *      standard form: G rows negated, a ranged row [lo, hi] as a.x <= hi and
+ *      -a.x <= -lo (an equality when lo == hi).  Host code only: reading needs no GPU. */
+typedef struct b2p_mps b2p_mps;
+/* Reads `path`; on failure returns B2P_INVALID_ARGUMENT with the reason and line in err. */
+int  b2p_mps_read(const char* path, b2p_mps** out, char* err, size_t errlen);
+void b2p_mps_free(b2p_mps* mps);
+/* Sizes: m rows (objective excluded), n columns, nnz; objective sense and offset; the
+ * standard form's rows and nonzeros.  Any pointer may be null. */
+int  b2p_mps_dims(const b2p_mps* mps, int* m, int* n, int64_t* nnz, int* maximize, double* obj_offset, int* std_m,
+                  int64_t* std_nnz);
+/* The model as read: CSR of the rows (column indices ascending), row_type 'L' / 'G' / 'E',
+ * ranged flag, rhs (a ranged row's lower end), range upper end; per column cost, bounds and
+ * kind (0 continuous, 1 integer, 2 binary).  Any pointer may be null. */
+int  b2p_mps_model(const b2p_mps* mps, int32_t* rowptr, int32_t* colidx, double* vals, char* row_type,
+                   uint8_t* ranged, double* rhs, double* range_upper, double* obj, double* lb, double* ub,
+                   uint8_t* col_type);
+/* The standard form (std_m rows) in b2p_upload_lp's layout; c is negated for maximisation. */
+int  b2p_mps_standard_form(const b2p_mps* mps, int32_t* rowptr, int32_t* colidx, double* vals, double* b,
+                           double* c, double* lb, double* ub, uint8_t* is_eq);
+/* b2p_upload_lp of the standard form. */
+int  b2p_upload_mps(void* ctx, const b2p_mps* mps);
+
 /* Per-kernel timing of the Halpern iteration on the uploaded LP, after a
  * b2p_solve with the same params: `reps` plain iterations launched one kernel
  * at a time between CUDA events on the context stream.  Returns the mean

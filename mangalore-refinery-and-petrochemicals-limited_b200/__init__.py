@@ -94,6 +94,15 @@ SIGNATURES = {
                                    _F64P, _F64P, _F64P, _U8P]),
     "b2p_batch_solve": (C.c_int, [_P, C.POINTER(Params), _P, _P, _P, _P, _P, _P, _P, _P, _P, C.POINTER(Result)]),
     "b2p_batch_objectives": (C.c_int, [_P, _P, _P, _P]),
+    "b2p_mps_read": (C.c_int, [C.c_char_p, C.POINTER(C.c_void_p), C.c_char_p, C.c_size_t]),
+    "b2p_mps_free": (None, [_P]),
+    "b2p_mps_dims": (C.c_int, [_P, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int64),
+                               C.POINTER(C.c_int), C.POINTER(C.c_double), C.POINTER(C.c_int),
+                               C.POINTER(C.c_int64)]),
+    "b2p_mps_model": (C.c_int, [_P, _I32P, _I32P, _F64P, C.c_char_p, _U8P, _F64P, _F64P, _F64P, _F64P, _F64P,
+                                _U8P]),
+    "b2p_mps_standard_form": (C.c_int, [_P, _I32P, _I32P, _F64P, _F64P, _F64P, _F64P, _F64P, _U8P]),
+    "b2p_upload_mps": (C.c_int, [_P, _P]),
     "b2p_mlp_create": (C.c_int, [_P, C.c_int, C.c_int, C.c_int, C.c_uint64]),
     "b2p_mlp_train_epoch": (C.c_int, [_P, _F32P, _F32P, C.c_int, C.c_int, C.c_float, C.POINTER(C.c_float)]),
     "b2p_mlp_infer": (C.c_int, [_P, _F32P, C.c_int, _F32P]),
@@ -143,6 +152,61 @@ def device_info(device: int = 0) -> dict:
             "cc": (info.compute_capability_major, info.compute_capability_minor),
             "sm_count": info.multiprocessor_count, "l2_bytes": info.l2_cache_bytes,
             "message": info.status_message.decode()}
+
+
+class MpsFile:
+    """An MPS file read by the library (b2p_mps_read): its model as parsed, its
+    standard form, and the handle b2p_upload_mps takes.  Host code only; needs no GPU."""
+
+    def __init__(self, path):
+        self._h = C.c_void_p()
+        err = C.create_string_buffer(512)
+        st = lib().b2p_mps_read(str(path).encode(), C.byref(self._h), err, 512)
+        if st != OK:
+            raise B2PError(st, err.value.decode())
+        m, n, mx, sm = C.c_int(), C.c_int(), C.c_int(), C.c_int()
+        nnz, snnz = C.c_int64(), C.c_int64()
+        off = C.c_double()
+        lib().b2p_mps_dims(self._h, C.byref(m), C.byref(n), C.byref(nnz), C.byref(mx), C.byref(off), C.byref(sm),
+                           C.byref(snnz))
+        self.m, self.n, self.nnz, self.maximize, self.obj_offset = m.value, n.value, nnz.value, bool(mx.value), off.value
+        self.std_m, self.std_nnz = sm.value, snnz.value
+
+    def model(self) -> dict:
+        """Rows as parsed: CSR (columns ascending), row type 'L' / 'G' / 'E', ranged flag, rhs
+        (the lower end of a ranged row), range upper end; columns: cost, bounds, kind
+        (0 continuous, 1 integer, 2 binary)."""
+        m, n, z = self.m, self.n, self.nnz
+        out = dict(rowptr=np.zeros(m + 1, np.int32), colidx=np.zeros(z, np.int32), vals=np.zeros(z),
+                   row_type=C.create_string_buffer(m + 1), ranged=np.zeros(m, np.uint8), rhs=np.zeros(m),
+                   range_upper=np.zeros(m), obj=np.zeros(n), lb=np.zeros(n), ub=np.zeros(n),
+                   col_type=np.zeros(n, np.uint8))
+        lib().b2p_mps_model(self._h, *[out[k] for k in ("rowptr", "colidx", "vals", "row_type", "ranged", "rhs",
+                                                         "range_upper", "obj", "lb", "ub", "col_type")])
+        out["row_type"] = out["row_type"].raw[:m].decode()
+        return out
+
+    def standard_form(self):
+        """lpgen.StdLP of the file (ranged rows written as two <= rows)."""
+        from .lpgen import StdLP
+        m, n, z = self.std_m, self.n, self.std_nnz
+        a = dict(rowptr=np.zeros(m + 1, np.int32), colidx=np.zeros(z, np.int32), vals=np.zeros(z), b=np.zeros(m),
+                 c=np.zeros(n), lb=np.zeros(n), ub=np.zeros(n), is_eq=np.zeros(m, np.uint8))
+        lib().b2p_mps_standard_form(self._h, *[a[k] for k in ("rowptr", "colidx", "vals", "b", "c", "lb", "ub",
+                                                              "is_eq")])
+        return StdLP(m, n, a["rowptr"], a["colidx"], a["vals"], a["b"], a["c"], a["lb"], a["ub"], a["is_eq"],
+                     name="mps")
+
+    def close(self):
+        if self._h:
+            lib().b2p_mps_free(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def default_params(**kw) -> Params:
@@ -252,6 +316,11 @@ class Context:
                                         np.ascontiguousarray(lp.lb, np.float64),
                                         np.ascontiguousarray(lp.ub, np.float64),
                                         np.ascontiguousarray(lp.is_eq, np.uint8)))
+
+    def upload_mps(self, mps):
+        """Upload the standard form of an MpsFile (b2p_upload_mps)."""
+        self.m, self.n = int(mps.std_m), int(mps.n)
+        self._check(lib().b2p_upload_mps(self._h, mps._h))
 
     def solve(self, x0=None, y0=None, **params):
         p = default_params(**params)

@@ -196,13 +196,30 @@ __device__ __forceinline__ void block_sums(double (&v)[NV], double* sh /* [32*NV
 }
 
 // One lane's row of a SELL-32 slice: v / ix point at the lane's first entry, the
-// next entry of the same row is 32 elements further.  Sequential sum.
+// next entry of the same row is 32 elements further.  Sequential sum in entry order.
+// Entries are taken in batches of B (8 in FP32, 4 in FP64, the most the register
+// budget of two 512-thread CTAs per SM holds without spilling in the loop): every
+// value and index load of a batch (the last batch predicated on the row's length)
+// is issued before the first gather that needs one, so a slice of up to B entries
+// per lane costs one L2 round trip and a longer one a round trip per batch.
 template <typename MT>
 __device__ __forceinline__ MT ell_dot(const MT* __restrict__ v, const uint16_t* __restrict__ ix, int len,
                                       const MT* __restrict__ g) {
+    constexpr int B = sizeof(MT) == 4 ? 8 : 4;
     MT s = (MT)0;
-#pragma unroll 4
-    for (int q = 0; q < len; ++q) s += v[q * 32] * g[ix[q * 32]];
+    for (int q = 0; q < len; q += B) {
+        MT vv[B];
+        unsigned ii[B];
+#pragma unroll
+        for (int u = 0; u < B; ++u) {
+            const bool h = q + u < len;
+            vv[u] = h ? v[(q + u) * 32] : (MT)0;
+            ii[u] = h ? (unsigned)ix[(q + u) * 32] : 0u;
+        }
+#pragma unroll
+        for (int u = 0; u < B; ++u)
+            if (q + u < len) s += vv[u] * g[ii[u]];
+    }
     return s;
 }
 

@@ -10,6 +10,8 @@
 #include "test_harness.hpp"
 
 #include <bharatopt/benchmark_framework.hpp>
+#include <bharatopt/branch_and_bound.hpp>
+#include <bharatopt/milp_foundation.hpp>
 #include <bharatopt/dual_revised_simplex.hpp>
 #include <bharatopt/execution_router.hpp>
 #include <bharatopt/first_order_solver.hpp>
@@ -19,6 +21,8 @@
 #include <cmath>
 #include <string>
 
+#include "b200_branch_and_bound.hpp"
+#include "b200_router.hpp"
 #include "b2p_dropin.hpp"
 
 using namespace bharatopt;
@@ -165,4 +169,173 @@ TEST_CASE(DropIn_07_AdaptiveRouterPicksGpuAtScale) {
     RoutingDecision d = router.decide(model, f, est);
     EXPECT_EQ(d.execution_device, "GPU");
     EXPECT_EQ(d.solver_variant, "GPU_PDHG");
+}
+
+namespace {
+
+// A two-variable hand LP of the size of the reference's FO_* models.
+LPModel toy_model() {
+    LPModel model("toy_router");
+    model.set_sense(ObjectiveSense::MAXIMIZE);
+    index_t x = model.add_variable("x", 0.0, 10.0, 3.0);
+    index_t y = model.add_variable("y", 0.0, 10.0, 5.0);
+    model.add_constraint("c1", {{x, 1.0}, {y, 2.0}}, ConstraintSense::LESS_EQUAL, 8.0);
+    model.add_constraint("c2", {{x, 3.0}, {y, 1.0}}, ConstraintSense::LESS_EQUAL, 9.0);
+    return model;
+}
+
+// Features of the block-angular multi-period LP (204k rows, 1M columns, 8.2M nonzeros)
+// on top of the features of a small model.
+WorkloadFeatures block_angular_scale(WorkloadFeatures f) {
+    f.m = f.orig_m = f.reduced_m = 204000;
+    f.n = f.orig_n = f.reduced_n = 1000000;
+    f.nnz = f.orig_nnz = f.reduced_nnz = 8200000;
+    f.density = 8.2e6 / (2.04e5 * 1.0e6);
+    f.avg_nnz_per_row = 8.2e6 / 2.04e5;
+    f.avg_nnz_per_col = 8.2;
+    return f;
+}
+
+}  // namespace
+
+TEST_CASE(DropIn_08_CalibratedRouterKeepsToyModelsOnCpu) {
+    // the B200-calibrated estimates (not a size threshold) keep an FO-sized model on the CPU
+    B200ExecutionRouter router;
+    LPModel toy = toy_model();
+    WorkloadFeatures f = router.analyse(toy);
+    EXPECT_TRUE(f.gpu_available);
+    std::vector<CostEstimate> est = router.estimate(f);
+    RoutingDecision d = router.decide(toy, f, est);
+    EXPECT_EQ(d.execution_device, "CPU");
+    EXPECT_TRUE(d.routing_reason.rfind("B200_CALIBRATED_CPU_SELECTED", 0) == 0);
+    EXPECT_TRUE(d.predicted_gpu_cost_ms > d.predicted_cpu_cost_ms);
+    RoutedSolveResult r = router.solve(toy);
+    EXPECT_EQ(r.status, "OPTIMAL");
+    EXPECT_NEAR(r.objective_value, 3.0 * 2.0 + 5.0 * 3.0, 1e-6);
+}
+
+TEST_CASE(DropIn_09_CalibratedRouterPicksGpuAtBlockAngularScale) {
+    B200ExecutionRouter router;
+    LPModel toy = toy_model();
+    WorkloadFeatures big = block_angular_scale(router.analyse(toy));
+    std::vector<CostEstimate> est = router.estimate(big);
+    RoutingDecision d = router.decide(toy, big, est);
+    EXPECT_EQ(d.execution_device, "GPU");
+    EXPECT_EQ(d.solver_variant, "GPU_PDHG");
+    EXPECT_TRUE(d.routing_reason.rfind("B200_CALIBRATED_GPU_SELECTED", 0) == 0);
+    EXPECT_TRUE(d.predicted_gpu_cost_ms < d.predicted_cpu_cost_ms);
+    // the calibrated GPU estimate at this size: seconds, not the laptop formula's minutes
+    EXPECT_TRUE(d.predicted_gpu_cost_ms > 1000.0 && d.predicted_gpu_cost_ms < 20000.0);
+}
+
+TEST_CASE(RouterB200_01_NoDeviceStaysOnCpu) {
+    // without a usable device the calibrated router never selects the GPU path
+    B200ExecutionRouter router;
+    LPModel toy = toy_model();
+    WorkloadFeatures big = block_angular_scale(router.analyse(toy));
+    big.gpu_available = false;
+    big.cuda_available = false;
+    RoutingDecision d = router.decide(toy, big, router.estimate(big));
+    EXPECT_EQ(d.execution_device, "CPU");
+    EXPECT_TRUE(d.routing_reason.rfind("B200_CALIBRATED_GPU_UNAVAILABLE", 0) == 0);
+}
+
+namespace {
+
+// Small MILPs for the batched branch-and-bound, each solved by the reference's
+// BranchAndBoundEngine as well.
+LPModel milp_three_int() {
+    LPModel m("milp_three_int");
+    m.set_sense(ObjectiveSense::MAXIMIZE);
+    index_t x = m.add_variable("x", 0.0, 10.0, 5.0, VariableType::INTEGER);
+    index_t y = m.add_variable("y", 0.0, 10.0, 4.0, VariableType::INTEGER);
+    index_t z = m.add_variable("z", 0.0, 10.0, 3.0, VariableType::INTEGER);
+    m.add_constraint("r1", {{x, 2.0}, {y, 3.0}, {z, 1.0}}, ConstraintSense::LESS_EQUAL, 5.0);
+    m.add_constraint("r2", {{x, 4.0}, {y, 1.0}, {z, 2.0}}, ConstraintSense::LESS_EQUAL, 11.0);
+    m.add_constraint("r3", {{x, 3.0}, {y, 4.0}, {z, 2.0}}, ConstraintSense::LESS_EQUAL, 8.0);
+    return m;
+}
+
+LPModel milp_knapsack(int items, int rows, uint64_t seed) {
+    LPModel m("milp_knapsack_" + std::to_string(items));
+    m.set_sense(ObjectiveSense::MAXIMIZE);
+    uint64_t z = seed * 0x9E3779B97F4A7C15ull + 1;
+    auto next = [&]() {
+        z ^= z << 13;
+        z ^= z >> 7;
+        z ^= z << 17;
+        return (double)(z % 1000) / 1000.0;
+    };
+    std::vector<index_t> v;
+    for (int i = 0; i < items; ++i) v.push_back(m.add_variable("x" + std::to_string(i), 0.0, 1.0, 10.0 + 40.0 * next(),
+                                                              VariableType::BINARY));
+    for (int r = 0; r < rows; ++r) {
+        std::vector<std::pair<index_t, real_t>> t;
+        double total = 0.0;
+        for (int i = 0; i < items; ++i) {
+            const double w = 5.0 + 20.0 * next();
+            t.push_back({v[i], w});
+            total += w;
+        }
+        m.add_constraint("cap" + std::to_string(r), t, ConstraintSense::LESS_EQUAL, std::floor(0.4 * total));
+    }
+    return m;
+}
+
+LPModel milp_integer_infeasible() {
+    // the relaxation is feasible (x + y = 1.5), no integer point is
+    LPModel m("milp_integer_infeasible");
+    m.set_sense(ObjectiveSense::MINIMIZE);
+    index_t x = m.add_variable("x", 0.0, 5.0, 1.0, VariableType::INTEGER);
+    index_t y = m.add_variable("y", 0.0, 5.0, 2.0, VariableType::INTEGER);
+    m.add_constraint("half", {{x, 1.0}, {y, 1.0}}, ConstraintSense::EQUAL, 1.5);
+    return m;
+}
+
+LPModel milp_mixed() {
+    // integers and a continuous variable, a >= row and an equality
+    LPModel m("milp_mixed");
+    m.set_sense(ObjectiveSense::MINIMIZE);
+    index_t a = m.add_variable("a", 0.0, 20.0, 3.0, VariableType::INTEGER);
+    index_t b = m.add_variable("b", 0.0, 20.0, 2.0, VariableType::INTEGER);
+    index_t c = m.add_variable("c", 0.0, 10.0, 1.5, VariableType::CONTINUOUS);
+    m.add_constraint("cover", {{a, 2.0}, {b, 1.0}, {c, 1.0}}, ConstraintSense::GREATER_EQUAL, 7.5);
+    m.add_constraint("mix", {{a, 1.0}, {b, 3.0}}, ConstraintSense::GREATER_EQUAL, 5.5);
+    m.add_constraint("tie", {{a, 1.0}, {b, -1.0}, {c, 1.0}}, ConstraintSense::EQUAL, 0.5);
+    return m;
+}
+
+void expect_same_milp_answer(const LPModel& model) {
+    BranchAndBoundEngine ref;
+    BnBResult r = ref.solve(model);
+    B200BranchAndBound gpu;
+    BnBResult g = gpu.solve(model);
+    EXPECT_TRUE(g.status == r.status);
+    if (r.status == BnBSolverStatus::OPTIMAL && g.status == BnBSolverStatus::OPTIMAL) {
+        EXPECT_NEAR(g.objective_value, r.objective_value, 1e-4 * std::max(1.0, std::fabs(r.objective_value)));
+        IntegerVerificationResult v = MilpFoundation::verify_integer_feasibility(model, g.solution, 1e-5);
+        EXPECT_TRUE(v.is_integer_feasible);
+    }
+}
+
+}  // namespace
+
+TEST_CASE(DropIn_10_BatchedBnBMatchesReferenceEngine) {
+    expect_same_milp_answer(milp_three_int());
+    expect_same_milp_answer(milp_integer_infeasible());
+    expect_same_milp_answer(milp_mixed());
+    expect_same_milp_answer(milp_knapsack(12, 1, 3));
+}
+
+TEST_CASE(DropIn_11_BatchedBnBKnapsackFrontier) {
+    // 24 binaries under two capacity rows: many open nodes, solved a frontier per batch
+    LPModel model = milp_knapsack(24, 2, 7);
+    B200BranchAndBound gpu;
+    BnBResult g = gpu.solve(model);
+    BranchAndBoundEngine ref;
+    BnBResult r = ref.solve(model);
+    EXPECT_TRUE(g.status == BnBSolverStatus::OPTIMAL);
+    EXPECT_TRUE(r.status == BnBSolverStatus::OPTIMAL);
+    EXPECT_NEAR(g.objective_value, r.objective_value, 1e-4 * std::max(1.0, std::fabs(r.objective_value)));
+    EXPECT_TRUE(gpu.batches_solved() < g.telemetry.nodes_processed);  // several nodes per launch
 }

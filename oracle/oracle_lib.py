@@ -8,12 +8,15 @@ Neither is ever loaded by the product path.
 from __future__ import annotations
 
 import ctypes as C
+import os
 from pathlib import Path
 
 import numpy as np
 
 HERE = Path(__file__).resolve().parent
 REF_DIR = HERE / "_ref"
+# the reference source tree (its MPS fixtures are read by the CPU tests when it is present)
+REF_TREE = Path(os.environ.get("B2P_REFERENCE_TREE", "/root/reference"))
 
 _F64P = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
 _I32P = np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS")
@@ -114,6 +117,11 @@ class RefLib:
         L.ref_spmv_t.argtypes = [C.c_int, C.c_int, _I32P, _I32P, _F64P, _F64P, _F64P]
         L.ref_verify.argtypes = [C.POINTER(RefLP), _F64P, C.c_double, C.c_double, C.c_int,
                                  C.POINTER(RefVerifyResult)]
+        L.ref_mps_parse.restype = C.c_void_p
+        L.ref_mps_parse.argtypes = [C.c_char_p, C.c_char_p, C.c_int]
+        L.ref_mps_dims.argtypes = [C.c_void_p] + [C.POINTER(C.c_int)] * 4 + [C.POINTER(C.c_double)]
+        L.ref_mps_copy.argtypes = [C.c_void_p, _I32P, _I32P, _F64P, _I32P, _F64P, _F64P, _F64P, _F64P, _F64P, _I32P]
+        L.ref_mps_free.argtypes = [C.c_void_p]
         self.L = L
 
     @staticmethod
@@ -200,3 +208,23 @@ class RefLib:
                           0.0 if reported_obj is None else reported_obj, int(reported_obj is not None),
                           C.byref(out))
         return {k: getattr(out, k) for k, _ in RefVerifyResult._fields_}
+
+    def parse_mps(self, path):
+        """The reference MpsParser's LPModel of an MPS file, as arrays (rows in CSR with each
+        row's terms in the model's order; sense 0 <=, 1 =, 2 >=, 3 ranged)."""
+        err = C.create_string_buffer(512)
+        h = self.L.ref_mps_parse(str(path).encode(), err, 512)
+        if not h:
+            raise ValueError(err.value.decode())
+        m, n, nnz, mx, off = C.c_int(), C.c_int(), C.c_int(), C.c_int(), C.c_double()
+        self.L.ref_mps_dims(h, C.byref(m), C.byref(n), C.byref(nnz), C.byref(mx), C.byref(off))
+        out = dict(rowptr=np.zeros(m.value + 1, np.int32), colidx=np.zeros(nnz.value, np.int32),
+                   vals=np.zeros(nnz.value), sense=np.zeros(m.value, np.int32), rhs=np.zeros(m.value),
+                   range_upper=np.zeros(m.value), obj=np.zeros(n.value), lb=np.zeros(n.value), ub=np.zeros(n.value),
+                   vtype=np.zeros(n.value, np.int32))
+        self.L.ref_mps_copy(h, *[out[k] for k in ("rowptr", "colidx", "vals", "sense", "rhs", "range_upper", "obj",
+                                                   "lb", "ub", "vtype")])
+        self.L.ref_mps_free(h)
+        out.update(m=m.value, n=n.value, maximize=mx.value, obj_offset=off.value)
+        return out
+

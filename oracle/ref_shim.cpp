@@ -9,12 +9,16 @@
 //                        CSRMatrix::from_coo (src/sparse_matrix.cpp:59-111)
 //   ref_spmv/_t       -> CSRMatrix::multiply / multiply_transpose (src/sparse_matrix.cpp:153-185)
 //   ref_verify        -> SolutionVerifier::verify     (src/solution_verifier.cpp:42-204)
+//   ref_mps_*         -> MpsParser::parse_file        (src/mps_parser.cpp:140-531), the LPModel it
+//                        builds read out row by row
 #include <bharatopt/first_order_solver.hpp>
+#include <bharatopt/mps_parser.hpp>
 #include <bharatopt/presolve.hpp>
 #include <bharatopt/solution_verifier.hpp>
 #include <bharatopt/sparse_matrix.hpp>
 #include <bharatopt/lp_model.hpp>
 #include <chrono>
+#include <cstdio>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -225,5 +229,64 @@ int ref_verify(const RefLP* lp, const double* x, double feas_tol, double reporte
     out->violated_bounds = (long)r.violated_bound_count;
     return 0;
 }
+
+// ---- MPS through the reference's parser ----
+struct RefMps {
+    MpsParseResult res;
+};
+
+// Parses `path`; returns a handle (null on a parse failure, with the message in err).
+void* ref_mps_parse(const char* path, char* err, int errlen) {
+    MpsParser parser;
+    RefMps* h = new RefMps();
+    h->res = parser.parse_file(path);
+    if (h->res.status != MpsParseStatus::SUCCESS) {
+        if (err && errlen > 0) std::snprintf(err, errlen, "%s", h->res.error_message.c_str());
+        delete h;
+        return nullptr;
+    }
+    return h;
+}
+
+void ref_mps_dims(void* hv, int* m, int* n, int* nnz, int* maximize, double* obj_offset) {
+    const LPModel& md = ((RefMps*)hv)->res.model;
+    *m = (int)md.num_constraints();
+    *n = (int)md.num_variables();
+    size_t z = 0;
+    for (size_t i = 0; i < md.num_constraints(); ++i) z += md.get_constraint((index_t)i).terms.size();
+    *nnz = (int)z;
+    *maximize = md.sense() == ObjectiveSense::MAXIMIZE ? 1 : 0;
+    *obj_offset = md.obj_offset();
+}
+
+// Rows as CSR in each row's term order; sense 0 <=, 1 =, 2 >=, 3 ranged; variable type
+// 0 continuous, 1 integer, 2 binary.
+void ref_mps_copy(void* hv, int* rowptr, int* colidx, double* vals, int* sense, double* rhs, double* range_upper,
+                  double* obj, double* lb, double* ub, int* vtype) {
+    const LPModel& md = ((RefMps*)hv)->res.model;
+    rowptr[0] = 0;
+    for (size_t i = 0; i < md.num_constraints(); ++i) {
+        const Constraint& c = md.get_constraint((index_t)i);
+        int p = rowptr[i];
+        for (const auto& t : c.terms) {
+            colidx[p] = t.first;
+            vals[p++] = t.second;
+        }
+        rowptr[i + 1] = p;
+        sense[i] = c.sense == ConstraintSense::LESS_EQUAL ? 0 : c.sense == ConstraintSense::EQUAL ? 1
+                 : c.sense == ConstraintSense::GREATER_EQUAL ? 2 : 3;
+        rhs[i] = c.rhs;
+        range_upper[i] = c.range_upper;
+    }
+    for (size_t j = 0; j < md.num_variables(); ++j) {
+        const Variable& v = md.get_variable((index_t)j);
+        obj[j] = v.obj_coeff;
+        lb[j] = v.lower_bound;
+        ub[j] = v.upper_bound;
+        vtype[j] = v.type == VariableType::CONTINUOUS ? 0 : v.type == VariableType::INTEGER ? 1 : 2;
+    }
+}
+
+void ref_mps_free(void* hv) { delete (RefMps*)hv; }
 
 }  // extern "C"

@@ -42,6 +42,8 @@ def test_dropin_without_gpu_reports_unavailable():
     assert not unexpected, unexpected
     # every CPU-only test of the reference still passes next to the drop-in
     assert res["FirstOrder_19_MandatoryHandLP"] == "PASS"
+    # the B200-calibrated router never selects the GPU path without a device
+    assert res["RouterB200_01_NoDeviceStaysOnCpu"] == "PASS"
 
 
 @pytest.mark.gpu
@@ -52,7 +54,8 @@ def test_dropin_reference_tests_and_parity():
     for name in ("FirstOrder_23_CPUvsGPUComparison", "GpuFoundation_07_IdentitySpMV", "GpuFoundation_17_Norm",
                  "Router_06_AutomaticGpuFailureFallback", "Phase20_FirstOrderSolverIntegration",
                  "DropIn_02_GeneratedModelsBitIdentical", "DropIn_05_HalpernEngineVerified",
-                 "DropIn_07_AdaptiveRouterPicksGpuAtScale"):
+                 "DropIn_07_AdaptiveRouterPicksGpuAtScale", "DropIn_08_CalibratedRouterKeepsToyModelsOnCpu",
+                 "DropIn_09_CalibratedRouterPicksGpuAtBlockAngularScale", "RouterB200_01_NoDeviceStaysOnCpu"):
         assert res.get(name) == "PASS", name
 
 
