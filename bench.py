@@ -542,6 +542,8 @@ def run_learned_workload(args):
                      "worst_obj_err_solved": float(objs["obj_err"][ok].max()) if ok.any() else None,
                      "statuses": {str(v): int((per["status"] == v).sum()) for v in np.unique(per["status"])},
                      "kernel_ms": summ["kernel_time_ms"], "kernel_launches": summ["kernel_launches"]}
+        if name in ("learned", "fp64_cold"):
+            res[name]["trace"] = trace_summary(*ctx.batch_trace(), args.heldout)
         if name == "learned":
             res[name]["fallbacks"] = summ["fallbacks"]
             res[name]["warm_used"] = int(per["warm_used"].sum())
@@ -619,6 +621,23 @@ def run_learned_workload(args):
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
+
+
+def trace_summary(t_ms, active, count, sm_count=148):
+    """Where the time of one batched solve goes, from its active-instance trace: the
+    time by which 50 / 90 / 99 / 100 % of the instances had finished, and the share of
+    the solve spent with fewer active instances than SMs (the tail, where most SMs idle)."""
+    t = np.asarray(t_ms, float)
+    a = np.asarray(active, float)
+    out = {"points": int(len(t)), "total_ms": float(t[-1]) if len(t) else 0.0}
+    for q in (50, 90, 99, 100):
+        left = count * (1 - q / 100.0)
+        hit = np.nonzero(a <= left)[0]
+        out[f"t{q}_ms"] = float(t[hit[0]]) if len(hit) else None
+    if len(t) > 1 and t[-1] > 0:
+        dt = np.diff(t)
+        out["tail_share"] = float(dt[a[:-1] < sm_count].sum() / t[-1])
+    return out
 
 
 def read_profile(path):

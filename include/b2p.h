@@ -127,7 +127,9 @@ typedef struct {
                                        are absorbed by the bounds), the sum bounds how far below the
                                        optimum an infeasible x can reach to first order */
     double  eps_infeasible;         /* 1e-8: PDLP-style certificates from the fixed-point displacement
-                                       T(z) - z at every check.  Dual ray dy (primal infeasible): its ray
+                                       T(z) - z at the restart checks (every check in the single-LP
+                                       engine, every fourth in the batched one).  Dual ray dy (primal
+                                       infeasible): its ray
                                        objective -b.dy + sum_j min(a_j l_j, a_j u_j), a = A^T dy, is > 0
                                        and the violations of a on unbounded sides are <= eps_infeasible
                                        times it -> B2P_STATUS_INFEASIBLE_DETECTED.  Primal ray dx (dual
@@ -283,6 +285,13 @@ int b2p_batch_solve(void* ctx, const b2p_params* params, const double* x0, const
  * objective, src/branch_and_bound.cpp:517-537) -- and the FP64 bound on the
  * relative objective error of the answer (see b2p_params.eps_objective). */
 int b2p_batch_objectives(void* ctx, double* pobj_out, double* dobj_out, double* obj_err_out);
+
+/* Active-instance trace of the last batched solve (no reference counterpart): after
+ * every replay of the persistent-kernel graph (two chunk launches and their
+ * compactions) the host time in ms since the solve's first launch and the number of
+ * instances still running; a learned solve's cold fallback continues the trace.
+ * Writes up to `capacity` points and the total in *count. */
+int b2p_batch_trace(void* ctx, int capacity, int* count, double* t_ms, int32_t* active);
 
 /* ---- learned warm start: MLP in -> h -> h -> out, GELU, BF16 weights and
  *      activations, FP32 accumulation on the tcgen05 tensor cores ---- */

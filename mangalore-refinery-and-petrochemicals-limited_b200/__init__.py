@@ -94,6 +94,7 @@ SIGNATURES = {
                                    _F64P, _F64P, _F64P, _U8P]),
     "b2p_batch_solve": (C.c_int, [_P, C.POINTER(Params), _P, _P, _P, _P, _P, _P, _P, _P, _P, C.POINTER(Result)]),
     "b2p_batch_objectives": (C.c_int, [_P, _P, _P, _P]),
+    "b2p_batch_trace": (C.c_int, [_P, C.c_int, C.POINTER(C.c_int), _P, _P]),
     "b2p_mps_read": (C.c_int, [C.c_char_p, C.POINTER(C.c_void_p), C.c_char_p, C.c_size_t]),
     "b2p_mps_free": (None, [_P]),
     "b2p_mps_dims": (C.c_int, [_P, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int64),
@@ -378,6 +379,15 @@ class Context:
         p, d, e = np.zeros(cnt), np.zeros(cnt), np.zeros(cnt)
         self._check(lib().b2p_batch_objectives(self._h, _ptr(p), _ptr(d), _ptr(e)))
         return {"pobj": p, "dobj": d, "obj_err": e}
+
+    def batch_trace(self):
+        """(t_ms, active) after every persistent-graph replay of the last batched solve."""
+        n = C.c_int()
+        self._check(lib().b2p_batch_trace(self._h, 0, C.byref(n), None, None))
+        t = np.zeros(n.value)
+        a = np.zeros(n.value, np.int32)
+        self._check(lib().b2p_batch_trace(self._h, n.value, C.byref(n), _ptr(t), _ptr(a)))
+        return t, a
 
     def batch_solve_learned(self, features, fallback=True, outputs=True, **params):
         """Learned warm start for every instance of the uploaded batch (see

@@ -112,7 +112,13 @@ struct BatchWork {
     DBuf<double> ox, oy, oom;
     bool solved = false;
     int tuned_threads[2] = {0, 0};  // block size per precision (0 = not tuned yet)
+    int tuned_chunk[2] = {2048, 2048};  // iterations per chunk launch per precision
     DBuf<int32_t> list;             // instances re-initialised by a subset solve
+    // active-instance trace of the last solve: host time (ms from the first graph launch of
+    // the solve) and instances still active after each graph launch (a fallback run continues
+    // the same trace)
+    std::vector<double> trace_ms;
+    std::vector<int32_t> trace_active;
 };
 
 void batch_free(Ctx* ctx) {
@@ -222,6 +228,11 @@ __device__ __forceinline__ MT ell_dot(const MT* __restrict__ v, const uint16_t* 
     }
     return s;
 }
+
+// Slice of round r for warp w of nw: rounds alternate the direction in which the
+// (length-sorted) slices are dealt, w then nw - 1 - w, so every warp's share of long
+// and short slices is even.  Increasing in r for a fixed warp.
+__device__ __forceinline__ int snake_slice(int r, int w, int nw) { return r * nw + ((r & 1) ? nw - 1 - w : w); }
 
 // The 32 rows of one slice summed by the whole warp over the CSR copy (rows
 // first .. first+cnt-1, global numbering; `off` localises the column index).
@@ -506,8 +517,10 @@ __device__ __forceinline__ void batch_chunk_body(const BArgs& a, int chunk) {
             const MT tau = (MT)(eta / om), sigma = (MT)(eta * om);
             const MT wk = (MT)((kk + 1.0) / (kk + 2.0)), wa = (MT)(1.0 / (kk + 2.0));
             double acc[4] = {0, 0, 0, 0};  // |x - T(x)|^2 and |y - T(y)|^2 (first or check), distances to anchors
-            // ---- primal phase: one thread per column, gathers y from shared memory
-            for (int sl = warp; sl < ncs; sl += nwarps) {
+            // ---- primal phase: one thread per column, gathers y from shared memory; slices
+            // (longest first) are dealt to the warps boustrophedon-wise, which evens out the
+            // warps' load round trips before the barrier
+            for (int r = 0, sl = warp; sl < ncs; ++r, sl = snake_slice(r, warp, nwarps)) {
                 const int j = (sl << 5) + lane;
                 const bool valid = j < n;
                 ColP<MT> p;
@@ -540,7 +553,7 @@ __device__ __forceinline__ void batch_chunk_body(const BArgs& a, int chunk) {
             }
             __syncthreads();
             // ---- dual phase: one thread per row, gathers xh from shared memory
-            for (int sl = warp; sl < nrs; sl += nwarps) {
+            for (int r = 0, sl = warp; sl < nrs; ++r, sl = snake_slice(r, warp, nwarps)) {
                 const int i = (sl << 5) + lane;
                 const bool valid = i < m;
                 RowP<MT> p;
@@ -1003,7 +1016,7 @@ std::string batch_key(BatchWork* w, int precision) {
     double mean_m = (double)w->inst_m / w->count, mean_n = (double)w->inst_n / w->count;
     double nnz_col = (double)w->nnz / std::max<int64_t>(w->tot_n, 1);
     std::ostringstream os;
-    os << "batch3_p" << precision << "_c" << (int)std::log2(std::max(1, w->count)) << "_m"
+    os << "batch4_p" << precision << "_c" << (int)std::log2(std::max(1, w->count)) << "_m"
        << (int)std::log2(mean_m + 1) << "_n" << (int)std::log2(mean_n + 1) << "_k" << (int)std::lround(nnz_col) << "_M"
        << w->max_m << "_N" << w->max_n << "_shared" << (w->nmat == 1 && w->count > 1);
     return os.str();
@@ -1124,8 +1137,13 @@ int init_instances(Ctx* ctx, BatchWork* w, const b2p_params* p, const double* x0
 }
 
 // Times each block size on a size-stratified sample of the batch (no termination,
-// fixed iteration count, no re-centring); instance state is re-initialised
-// afterwards by the caller.
+// fixed iteration count, no re-centring), then the chunk length: with the chosen block
+// size, launches of a and 4a iterations give the per-iteration cost p and the fixed
+// cost o of a chunk (launch, loading and storing every instance's state, plus the
+// compaction that follows); the chunk is the shortest power of two from 256 to 8192
+// whose fixed cost is at most 2 % of its iterations -- shorter chunks drop finished
+// instances sooner, so the tail of an uneven batch is cut finer.  Instance state is
+// re-initialised afterwards by the caller.
 template <typename MT>
 int autotune(Ctx* ctx, BatchWork* w, const b2p_params* p, TuneCfg* best) {
     std::string key = batch_key(w, sizeof(MT) == 8 ? 0 : 1);
@@ -1145,31 +1163,48 @@ int autotune(Ctx* ctx, BatchWork* w, const b2p_params* p, TuneCfg* best) {
     float best_ms = 1e30f;
     *best = {256, 2048};
     size_t sm = smem_bytes(w, sizeof(MT));
-    for (int th : {128, 256, 512}) {
+    auto fn = k_batch_chunk<MT>;
+    B2P_CUDA(ctx, cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    // one trial launch of `iters` iterations over the sample with `th` threads (ms; < 0: the
+    // block size does not fit)
+    auto trial = [&](int th, int iters, float* ms) -> int {
+        *ms = -1.0f;
         int st = init_instances<MT>(ctx, w, &tp, nullptr, nullptr, nullptr);
         if (st) return st;
         int32_t cnt[2] = {0, sample};
         B2P_CUDA(ctx, cudaMemcpyAsync(w->counters.p, cnt, sizeof(cnt), cudaMemcpyHostToDevice, s));
         BArgs a = make_args<MT>(w, &tp, dids.p);
-        auto fn = k_batch_chunk<MT>;
-        B2P_CUDA(ctx, cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
         int per_sm = 0;
         B2P_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, th, sm));
-        if (per_sm < 1) continue;
+        if (per_sm < 1) return B2P_OK;
         int grid = std::min(sample, ctx->sm_count * per_sm);
         cudaEventRecord(ctx->ev0, s);
-        fn<<<grid, th, sm, s>>>(a, trial_iters);
+        fn<<<grid, th, sm, s>>>(a, iters);
+        k_batch_compact<<<1, 1024, 0, s>>>(w->ictrl.p, dids.p, w->active2.p, w->counters.p);
         cudaEventRecord(ctx->ev1, s);
         B2P_LAUNCH(ctx);
         B2P_CUDA(ctx, cudaEventSynchronize(ctx->ev1));
         ctx->launches += 2;
-        float ms = 0;
-        cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
-        if (ms < best_ms) {
+        cudaEventElapsedTime(ms, ctx->ev0, ctx->ev1);
+        return B2P_OK;
+    };
+    for (int th : {128, 256, 512}) {
+        float ms = 0.0f;
+        int st = trial(th, trial_iters, &ms);
+        if (st) return st;
+        if (ms >= 0.0f && ms < best_ms) {
             best_ms = ms;
-            *best = {th, 2048};
+            best->threads = th;
         }
     }
+    float t4 = 0.0f;
+    int st = trial(best->threads, 4 * trial_iters, &t4);
+    if (st) return st;
+    const double per_iter = std::max(1e-9, (double)(t4 - best_ms) / (3.0 * trial_iters));
+    const double fixed = std::max(0.0, (double)best_ms - trial_iters * per_iter);
+    int chunk = 256;
+    while (chunk < 8192 && fixed > 0.02 * chunk * per_iter) chunk *= 2;
+    best->chunk = chunk;
     cache_store(key, *best);
     return B2P_OK;
 }
@@ -1199,6 +1234,7 @@ int batch_run(Ctx* ctx, BatchWork* w, const b2p_params* p, const double* x0_dev,
     TuneCfg cfg = {256, 2048};
     if (w->tuned_threads[prec] > 0) {
         cfg.threads = w->tuned_threads[prec];
+        cfg.chunk = w->tuned_chunk[prec];
     } else {
         if (subset) {
             ctx->err = "subset solve before a full solve of this precision";
@@ -1207,6 +1243,7 @@ int batch_run(Ctx* ctx, BatchWork* w, const b2p_params* p, const double* x0_dev,
         int st = autotune<MT>(ctx, w, p, &cfg);
         if (st) return st;
         w->tuned_threads[prec] = cfg.threads;
+        w->tuned_chunk[prec] = cfg.chunk;
     }
     // displacement buffers of the infeasibility certificates (sized for FP64, read as MT)
     if (p->eps_infeasible > 0.0) {
@@ -1324,11 +1361,21 @@ int batch_run(Ctx* ctx, BatchWork* w, const b2p_params* p, const double* x0_dev,
     cudaEventRecord(ctx->ev0, s);
     // no more than one instance per SM left: the wide form
     bool wide = have_wide && n_act <= ctx->sm_count;
+    const double trace_base = subset && !w->trace_ms.empty() ? w->trace_ms.back() : 0.0;
+    if (!subset) {
+        w->trace_ms.clear();
+        w->trace_active.clear();
+    }
+    const double t_loop = now_ms();
+    w->trace_ms.push_back(trace_base);
+    w->trace_active.push_back(n_act);
     while (graphs < max_graphs) {
         B2P_CUDA(ctx, cudaGraphLaunch(wide ? exec_w : exec, s));
         graphs++;
         B2P_CUDA(ctx, cudaMemcpyAsync(host_cnt, w->counters.p, 2 * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
         B2P_CUDA(ctx, cudaStreamSynchronize(s));
+        w->trace_ms.push_back(trace_base + now_ms() - t_loop);
+        w->trace_active.push_back(host_cnt[1]);
         if (host_cnt[1] == 0) break;
         if (have_wide && host_cnt[1] <= ctx->sm_count) wide = true;
         if (tl > 0 && now_ms() - t_start > tl) {
@@ -1720,6 +1767,24 @@ int b2p_batch_solve(void* p, const b2p_params* params, const double* x0, const d
     if (summary) {
         summary->solve_time_ms = now_ms() - t0;
         summary->kernel_launches = ctx->launches - l0;
+    }
+    return B2P_OK;
+}
+
+int b2p_batch_trace(void* p, int capacity, int* count, double* t_ms, int32_t* active) {
+    Ctx* ctx = static_cast<Ctx*>(p);
+    if (!ctx) return B2P_GPU_UNINITIALIZED;
+    BatchWork* w = ctx->bw;
+    if (!w || !w->solved) {
+        ctx->err = "b2p_batch_trace: no batched solve to report";
+        return B2P_NO_LP;
+    }
+    const int n = (int)w->trace_ms.size();
+    if (count) *count = n;
+    const int k = std::min(n, std::max(capacity, 0));
+    for (int i = 0; i < k; ++i) {
+        if (t_ms) t_ms[i] = w->trace_ms[i];
+        if (active) active[i] = w->trace_active[i];
     }
     return B2P_OK;
 }

@@ -5,3 +5,9 @@
 #include "../../include/b2p.h"
 
 extern "C" void bharatopt_b200_set_engine(const b2p_params* params);
+
+// Extension point (no reference counterpart): 1 selects the direct setup of
+// bharatopt::GPUFirstOrderSolver (one threaded pass from the model's rows to the
+// standard form, no validator / presolve, the Halpern engine), 0 the reference's front
+// end, -1 the B2P_SETUP environment variable (B2P_SETUP=direct).
+extern "C" void bharatopt_b200_set_setup(int direct);

@@ -18,7 +18,9 @@
 #include <bharatopt/gpu_backend.hpp>
 #include <bharatopt/solution_verifier.hpp>
 
+#include <chrono>
 #include <cmath>
+#include <cstdio>
 #include <string>
 
 #include "b200_branch_and_bound.hpp"
@@ -338,4 +340,100 @@ TEST_CASE(DropIn_11_BatchedBnBKnapsackFrontier) {
     EXPECT_TRUE(r.status == BnBSolverStatus::OPTIMAL);
     EXPECT_NEAR(g.objective_value, r.objective_value, 1e-4 * std::max(1.0, std::fabs(r.objective_value)));
     EXPECT_TRUE(gpu.batches_solved() < g.telemetry.nodes_processed);  // several nodes per launch
+}
+
+namespace {
+
+// Random sparse LP in the model API: m rows (<= and >=, and with `ranged` every third row
+// ranged), n columns in [0, 10], about k nonzeros per column, feasible at x0 = 1.
+LPModel random_model(int m, int n, int k, uint64_t seed, bool ranged) {
+    LPModel model("direct_setup_" + std::to_string(m));
+    uint64_t z = seed * 0x9E3779B97F4A7C15ull + 7;
+    auto u01 = [&]() {
+        z ^= z << 13;
+        z ^= z >> 7;
+        z ^= z << 17;
+        return (double)(z >> 11) * (1.0 / 9007199254740992.0);
+    };
+    std::vector<index_t> v(n);
+    for (int j = 0; j < n; ++j) v[j] = model.add_variable("x" + std::to_string(j), 0.0, 10.0, 2.0 * u01() - 1.0);
+    std::vector<std::vector<std::pair<index_t, real_t>>> rows(m);
+    for (int j = 0; j < n; ++j)
+        for (int q = 0; q < k; ++q) {
+            auto& r = rows[(size_t)(u01() * m) % m];
+            if (r.empty() || r.back().first != v[j]) r.push_back({v[j], 0.5 + u01()});  // no repeated term
+        }
+    for (int i = 0; i < m; ++i) {
+        double act = 0.0;
+        for (auto& t : rows[i]) act += t.second;
+        if (i % 3 == 0 || (!ranged && i % 3 == 2))
+            model.add_constraint("r" + std::to_string(i), rows[i], ConstraintSense::LESS_EQUAL, act + 1.0);
+        else if (i % 3 == 1)
+            model.add_constraint("r" + std::to_string(i), rows[i], ConstraintSense::GREATER_EQUAL, act - 1.0);
+        else {
+            index_t c = model.add_constraint("r" + std::to_string(i), ConstraintSense::RANGED, act - 0.5, act + 0.5);
+            for (auto& t : rows[i]) model.set_coeff(c, t.first, t.second);
+        }
+    }
+    return model;
+}
+
+double ms_since(std::chrono::high_resolution_clock::time_point t) {
+    return std::chrono::duration<double, std::milli>(std::chrono::high_resolution_clock::now() - t).count();
+}
+
+}  // namespace
+
+TEST_CASE(DropIn_12_DirectSetupMatchesAndSkipsHostPresolve) {
+    // same LP through the reference front end and through the direct setup, Halpern FP64
+    b2p_params p;
+    b2p_params_default(&p);
+    p.engine = B2P_ENGINE_HALPERN;
+    p.precision = B2P_FP64;
+    p.eps_rel_kkt = 1e-9;
+    p.max_iterations = 400000;
+    bharatopt_b200_set_engine(&p);
+    LPModel small = random_model(300, 900, 3, 11, false);
+    FirstOrderSolverOptions o;
+    o.backend_type = FirstOrderBackendType::GPU_FIRST_ORDER;
+    o.max_iterations = 400000;
+    bharatopt_b200_set_setup(0);
+    FirstOrderSolverResult a = FirstOrderLPSolver(o).solve(small);
+    bharatopt_b200_set_setup(1);
+    FirstOrderSolverResult b = FirstOrderLPSolver(o).solve(small);
+    EXPECT_EQ(a.status, FirstOrderSolverStatus::OPTIMAL);
+    EXPECT_EQ(b.status, FirstOrderSolverStatus::OPTIMAL);
+    EXPECT_NEAR(b.objective_value, a.objective_value, 1e-6 * std::max(1.0, std::fabs(a.objective_value)));
+    SolutionVerifier ver;
+    VerificationOptions vo;
+    vo.feasibility_tolerance = 1e-5;
+    EXPECT_TRUE(ver.verify(small, b.primal_solution, vo).verified);
+    // ranged rows: the direct setup keeps both ends (the reference front end keeps only the
+    // lower end), judged by the reference's verifier, which reads both
+    LPModel rng = random_model(300, 900, 3, 13, true);
+    FirstOrderSolverResult e = FirstOrderLPSolver(o).solve(rng);
+    EXPECT_EQ(e.status, FirstOrderSolverStatus::OPTIMAL);
+    vo.check_objective = false;
+    EXPECT_TRUE(ver.verify(rng, e.primal_solution, vo).verified);
+    // setup time at 800k nonzeros: a few iterations so the host front end dominates
+    LPModel big = random_model(20000, 100000, 8, 12, false);
+    p.max_iterations = 64;
+    p.eps_rel_kkt = 0.0;
+    bharatopt_b200_set_engine(&p);
+    o.max_iterations = 64;
+    bharatopt_b200_set_setup(0);
+    auto t0 = std::chrono::high_resolution_clock::now();
+    FirstOrderSolverResult c = FirstOrderLPSolver(o).solve(big);
+    const double ref_ms = ms_since(t0);
+    bharatopt_b200_set_setup(1);
+    t0 = std::chrono::high_resolution_clock::now();
+    FirstOrderSolverResult d = FirstOrderLPSolver(o).solve(big);
+    const double direct_ms = ms_since(t0);
+    bharatopt_b200_set_setup(-1);
+    bharatopt_b200_set_engine(nullptr);
+    std::printf("  [direct setup] 20000 x 100000, 800k nnz: reference front end + 64 iterations %.1f ms, "
+                "direct setup + 64 iterations %.1f ms\n", ref_ms, direct_ms);
+    EXPECT_EQ(c.status, FirstOrderSolverStatus::MAX_ITERATIONS);
+    EXPECT_EQ(d.status, FirstOrderSolverStatus::MAX_ITERATIONS);
+    EXPECT_TRUE(direct_ms * 2.0 < ref_ms);
 }

@@ -55,7 +55,9 @@ def test_dropin_reference_tests_and_parity():
                  "Router_06_AutomaticGpuFailureFallback", "Phase20_FirstOrderSolverIntegration",
                  "DropIn_02_GeneratedModelsBitIdentical", "DropIn_05_HalpernEngineVerified",
                  "DropIn_07_AdaptiveRouterPicksGpuAtScale", "DropIn_08_CalibratedRouterKeepsToyModelsOnCpu",
-                 "DropIn_09_CalibratedRouterPicksGpuAtBlockAngularScale", "RouterB200_01_NoDeviceStaysOnCpu"):
+                 "DropIn_09_CalibratedRouterPicksGpuAtBlockAngularScale", "RouterB200_01_NoDeviceStaysOnCpu",
+                 "DropIn_10_BatchedBnBMatchesReferenceEngine", "DropIn_11_BatchedBnBKnapsackFrontier",
+                 "DropIn_12_DirectSetupMatchesAndSkipsHostPresolve"):
         assert res.get(name) == "PASS", name
 
 

@@ -195,3 +195,21 @@ def test_planning_heldout_judge_learned(ctx, lpgen, b2p, reflib):
     s0, B, Cc, LB, UB, EQ = fam.standard_batch(P)
     summ, per, x, y = ws.solve(P, eps=1e-6, eps_objective=1e-6, max_iterations=400000)
     _planning_judge(per, x, y, fam, P, s0, B, Cc, LB, UB, EQ, lpgen, reflib, g["objectives"], 1e-6)
+
+
+def test_batch_autotuned_shape(ctx, lpgen, tmp_path, monkeypatch):
+    """The batched autotuner picks the CTA size and the chunk length (iterations per
+    persistent launch, a power of two in [256, 8192] whose fixed cost is <= 2 % of its
+    iterations); the summary reports threads * 1e5 + chunk, and a second solve of the
+    same precision reuses the tuned shape."""
+    monkeypatch.setenv("B2P_AUTOTUNE_CACHE", str(tmp_path / "tune.txt"))
+    lps = lpgen.uneven_batch(40, m_hi=500, seed=44)
+    upload_lps(ctx, lps)
+    summ, per, _, _ = ctx.batch_solve(precision="fp32", eps=1e-6, max_iterations=100000, outputs=False)
+    threads, chunk = divmod(int(round(summ["step_size"])), 100000)
+    assert threads in (128, 256, 512)
+    assert 256 <= chunk <= 8192 and chunk & (chunk - 1) == 0
+    assert np.all(per["status"] == 0)
+    summ2, per2, _, _ = ctx.batch_solve(precision="fp32", eps=1e-6, max_iterations=100000, outputs=False)
+    assert summ2["step_size"] == summ["step_size"]
+    assert np.array_equal(per2["iterations"], per["iterations"])  # deterministic
