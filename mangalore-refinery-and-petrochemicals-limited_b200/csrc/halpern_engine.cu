@@ -1,13 +1,13 @@
 // Halpern engine: restarted Halpern PDHG with reflection on a diagonally scaled LP.
 //
-// Precision: B2P_FP64 keeps everything in FP64.  B2P_FP32 (mixed) stores the
-// scaled matrix values (the bytes that dominate an iteration) and the gathered
-// operand xh of A xh in FP32, while the Halpern iterates x, y, their anchors,
-// the y gathered by A^T y, every accumulation, the scaling, the restart
-// residuals and the KKT stay FP64.  Measured on the random-sparse family:
-// FP32 iterates cost 1.8-3x more iterations and an FP32 copy of y for the A^T y
-// gather stalls convergence (the reduced costs c + A^T y cancel); FP32 values
-// and an FP32 xh cost none.
+// Precision: B2P_FP64 keeps everything in FP64.  B2P_FP32 (mixed) runs the
+// iteration in FP32 -- scaled matrix values, the Halpern iterates x, y, their
+// anchors and T(z), the problem vectors c, l, u, b and the dual bound, the SpMV
+// sums and the vector updates -- while FP64 is kept for the Ruiz / Pock-Chambolle
+// scaling factors, the squared-residual reductions that drive restarts, the KKT of
+// the original LP, and the iterative refinement: at every restart the LP is
+// re-centred on the current point (exact FP64 residuals b - A x, c + A^T y from
+// the original matrix), so the FP32 iterates only ever carry a correction.
 //
 // Problem (standard form of src/first_order_solver.cpp:68-101):
 //   min c.x  s.t. (Ax)_i <= b_i (<= rows) / = b_i (= rows),  l <= x <= u,
@@ -130,11 +130,12 @@ struct HalpernWork {
     DBuf<double> sv64, stv64;      // scaled A and A^T, FP64 (KKT, power iteration, FP64 engine)
     DBuf<float> sv32, stv32;       // scaled A and A^T, FP32 (FP32 engine)
     DBuf<double> c64, b64, l64, u64;
-    DBuf<double> x, xa, xt, y, ya, yt;  // FP64 iterates (both precisions)
+    DBuf<float> c32, b32, l32, u32, ylb32;  // the same in FP32 (mixed engine)
+    DBuf<double> x, xa, xt, y, ya, yt;  // iterates, sized for FP64; the mixed engine stores FP32 in them
     DBuf<double> xd, yd;                 // T(z) - z of the last check (infeasibility certificates)
     bool rays = false;                   // certificates on for the current solve
     DBuf<double> xh64;                   // gathered operand, FP64 engine
-    DBuf<float> xh32, yg32;              // gathered operands, mixed engine
+    DBuf<float> xh32;                    // gathered operand of A xh, mixed engine
     // FP64 re-centring: current centre in the original space, A xbar, A^T ybar, shifted dual bound
     bool recenter = false;
     DBuf<double> xbar, ybar, axbar, atybar, ylb_s;
@@ -280,47 +281,49 @@ __global__ void k_pow_init(int n, double* __restrict__ v) {
 }
 
 // ------------------------------------------------------------------ iterate init
-// x, xa, xt <- clamp(x0 / dc) ; y, ya, yt <- P_Y(y0 / dr) (warm start given in original space)
+// x, xa, xt <- clamp(x0 / dc) ; y, ya, yt <- P_Y(y0 / dr) (warm start given in original space;
+// ZT: the iterates' storage type)
+template <typename ZT>
 __global__ void k_init_iterates(int m, int n, const double* __restrict__ l, const double* __restrict__ u,
                                 const double* __restrict__ x0, const double* __restrict__ y0,
                                 const double* __restrict__ dr, const double* __restrict__ dc,
-                                const uint8_t* __restrict__ is_eq, const double* __restrict__ ylb, double* x,
-                                double* xa, double* xt, double* y, double* ya, double* yt, float* yg32) {
+                                const uint8_t* __restrict__ is_eq, const double* __restrict__ ylb, ZT* x, ZT* xa,
+                                ZT* xt, ZT* y, ZT* ya, ZT* yt) {
     int tid = blockIdx.x * blockDim.x + threadIdx.x, st = gridDim.x * blockDim.x;
     for (int j = tid; j < n; j += st) {
         double v = x0 ? x0[j] / dc[j] : 0.0;
         v = clampT(v, l[j], u[j]);
-        x[j] = v; xa[j] = v; xt[j] = v;
+        x[j] = (ZT)v; xa[j] = (ZT)v; xt[j] = (ZT)v;
     }
     for (int i = tid; i < m; i += st) {
         double v = y0 ? y0[i] / dr[i] : 0.0;
         const double lbv = ylb ? ylb[i] : 0.0;
         if (!is_eq[i] && v < lbv) v = lbv;
-        y[i] = v; ya[i] = v; yt[i] = v;
-        if (yg32) yg32[i] = (float)v;
+        y[i] = (ZT)v; ya[i] = (ZT)v; yt[i] = (ZT)v;
     }
 }
 
 // ------------------------------------------------------------------ iteration kernels
 enum { M_PLAIN = 0, M_FIRST = 1, M_CHECK = 2 };
 
-// VT: storage type of the matrix values and of xh (float: mixed, double: FP64).
-// GT: type of the gathered operand (primal: y, always FP64; dual: xh, VT).
+// VT: the iteration's type (float: mixed, double: FP64) -- matrix values, iterates,
+// problem vectors, sums and updates.  GT: type of the gathered operand (y for the
+// primal kernel, xh for the dual kernel), VT in both engines.
 template <typename VT, typename GT>
 struct IterArgs {
     const int32_t* ptr;    // CSR of the operator this kernel applies (A^T for primal, A for dual)
     const int32_t* idx;
     const VT* val;
     const GT* gather;      // y for the primal kernel, xh for the dual kernel
-    const double* cost;    // c (primal) / b (dual)
-    const double* lo;      // l (primal)
-    const double* hi;      // u (primal)
+    const VT* cost;        // c (primal) / b (dual)
+    const VT* lo;          // l (primal)
+    const VT* hi;          // u (primal)
     const uint8_t* is_eq;  // dual
-    const double* ylb;     // dual: lower bound of y on <= rows in scaled space (null = 0; refinement shifts it)
-    double* z;             // x or y, updated in place
+    const VT* ylb;         // dual: lower bound of y on <= rows in scaled space (null = 0; refinement shifts it)
+    VT* z;                 // x or y, updated in place
     VT* zh;                // primal: xh out (dual: unused)
-    const double* za;      // anchor
-    double* zt;            // T(z) at check iterations
+    const VT* za;          // anchor
+    VT* zt;                // T(z) at check iterations
     double* zd;            // T(z) - z at check iterations (null = certificates off); dual: >= 0 on <= rows
     Ctrl* ctrl;
     int rows;
@@ -405,17 +408,17 @@ __device__ __forceinline__ void ld_stream_w(const int* p, int (&v)[W], unsigned 
 // neighbourhood of the operand vector (for structured LPs such as block-angular
 // ones, one block's slice stays in L1); the CTA size is part of the tuned shape.
 // All 32 lanes of a warp stay converged through the shuffles.  Sums and updates
-// are FP64; VT only sets the bytes streamed for values and xh.
+// are in VT; the restart residuals accumulate in FP64.
 template <typename VT, typename GT, int L, int R, int MODE, bool PRIMAL>
 __global__ void __launch_bounds__(1024) k_iter(IterArgs<VT, GT> a, int it) {
     const Ctrl* ctrl = a.ctrl;
     if (ctrl->done) return;
     const unsigned long long pol = evict_first_policy();
     const double kk = (double)(ctrl->k_base + it);
-    const double wk = (kk + 1.0) / (kk + 2.0);
-    const double wa = 1.0 / (kk + 2.0);
-    const double step = PRIMAL ? ctrl->tau : ctrl->sigma;
-    const double rho = a.rho;
+    const VT wk = (VT)((kk + 1.0) / (kk + 2.0));
+    const VT wa = (VT)(1.0 / (kk + 2.0));
+    const VT step = (VT)(PRIMAL ? ctrl->tau : ctrl->sigma);
+    const VT rho = (VT)a.rho;
     const int lane = threadIdx.x & 31;
     const int sub = lane & (L - 1);
     const int rpw = 32 / L;
@@ -438,19 +441,19 @@ __global__ void __launch_bounds__(1024) k_iter(IterArgs<VT, GT> a, int it) {
         }
         // the row's own vectors, prefetched with the row pointers (they are only needed
         // after the reduction, so their latency overlaps the matrix stream)
-        double zr[R], cst[R], lo[R], hi[R], zan[R];
+        VT zr[R], cst[R], lo[R], hi[R], zan[R];
 #pragma unroll
         for (int u = 0; u < R; ++u) {
             const bool lead = sub == 0 && r[u] < row1;
-            zr[u] = lead ? a.z[r[u]] : 0.0;
-            cst[u] = lead ? a.cost[r[u]] : 0.0;
-            zan[u] = lead ? a.za[r[u]] : 0.0;
+            zr[u] = lead ? a.z[r[u]] : (VT)0;
+            cst[u] = lead ? a.cost[r[u]] : (VT)0;
+            zan[u] = lead ? a.za[r[u]] : (VT)0;
             if (PRIMAL) {
-                lo[u] = lead ? a.lo[r[u]] : 0.0;
-                hi[u] = lead ? a.hi[r[u]] : 0.0;
+                lo[u] = lead ? a.lo[r[u]] : (VT)0;
+                hi[u] = lead ? a.hi[r[u]] : (VT)0;
             } else {
-                lo[u] = (lead && !a.is_eq[r[u]]) ? (a.ylb ? a.ylb[r[u]] : 0.0) : -INFINITY;
-                hi[u] = 0.0;
+                lo[u] = (lead && !a.is_eq[r[u]]) ? (a.ylb ? a.ylb[r[u]] : (VT)0) : (VT)(-INFINITY);
+                hi[u] = (VT)0;
             }
         }
         // the first two entries of every lane, all loads in flight together
@@ -465,16 +468,16 @@ __global__ void __launch_bounds__(1024) k_iter(IterArgs<VT, GT> a, int it) {
                 v[u][e] = h ? ld_stream(a.val + k, pol) : (VT)0;
                 c[u][e] = h ? ld_stream(a.idx + k, pol) : -1;
             }
-        double s[R];
+        VT s[R];
 #pragma unroll
         for (int u = 0; u < R; ++u) {
-            s[u] = (c[u][0] >= 0) ? (double)v[u][0] * (double)a.gather[c[u][0]] : 0.0;
-            if (c[u][1] >= 0) s[u] += (double)v[u][1] * (double)a.gather[c[u][1]];
+            s[u] = (c[u][0] >= 0) ? v[u][0] * (VT)a.gather[c[u][0]] : (VT)0;
+            if (c[u][1] >= 0) s[u] += v[u][1] * (VT)a.gather[c[u][1]];
         }
 #pragma unroll
         for (int u = 0; u < R; ++u)
             for (int k = k0[u] + sub + 2 * L; k < k1[u]; k += L)
-                s[u] += (double)ld_stream(a.val + k, pol) * (double)a.gather[ld_stream(a.idx + k, pol)];
+                s[u] += ld_stream(a.val + k, pol) * (VT)a.gather[ld_stream(a.idx + k, pol)];
 #pragma unroll
         for (int u = 0; u < R; ++u) {
 #pragma unroll
@@ -484,24 +487,25 @@ __global__ void __launch_bounds__(1024) k_iter(IterArgs<VT, GT> a, int it) {
         for (int u = 0; u < R; ++u) {
             if (sub != 0 || r[u] >= row1) continue;
             const int row = r[u];
-            double zt;
+            VT zt;
             if (PRIMAL) {
                 zt = clampT(zr[u] - step * (cst[u] + s[u]), lo[u], hi[u]);
-                a.zh[row] = (VT)(2.0 * zt - zr[u]);
+                a.zh[row] = (VT)2 * zt - zr[u];
             } else {
                 zt = zr[u] + step * (s[u] - cst[u]);
                 if (zt < lo[u]) zt = lo[u];  // -inf on equality rows; NaN stays NaN
             }
-            const double za = zan[u];
-            a.z[row] = wk * ((1.0 + rho) * zt - rho * zr[u]) + wa * za;
+            const VT za = zan[u];
+            a.z[row] = wk * (((VT)1 + rho) * zt - rho * zr[u]) + wa * za;
             if (MODE != M_PLAIN) {
-                const double d = zr[u] - zt;
+                const double d = (double)zr[u] - (double)zt;
                 acc_r += d * d;
             }
             if (MODE == M_CHECK) {
                 a.zt[row] = zt;
-                if (a.zd) a.zd[row] = (!PRIMAL && lo[u] != -INFINITY) ? fmax(zt - zr[u], 0.0) : zt - zr[u];
-                const double e = zt - za;
+                const double dz = (double)zt - (double)zr[u];
+                if (a.zd) a.zd[row] = (!PRIMAL && lo[u] != (VT)(-INFINITY)) ? fmax(dz, 0.0) : dz;
+                const double e = (double)zt - (double)za;
                 acc_d += e * e;
             }
         }
@@ -519,7 +523,7 @@ __global__ void __launch_bounds__(1024) k_iter(IterArgs<VT, GT> a, int it) {
 // of W indices per lane (the warp reads 32 W contiguous elements of each).  Two
 // chunks are loaded before either is consumed.  The row's own vectors are read
 // with the slice offsets, coalesced (internal numbering).  Each CTA owns a
-// contiguous range of slices.  Sums and updates are FP64.
+// contiguous range of slices.  Sums and updates in VT.
 // WIN: the CTA first copies its window of the gathered vector (k_win_setup) into
 // shared memory and serves the gathers that fall inside it from there -- a random
 // 32-lane gather costs a few shared-memory bank cycles instead of 32 L1 requests.
@@ -571,10 +575,10 @@ __global__ void __launch_bounds__(1024) k_iter_sell(IterArgs<VT, GT> a, int it) 
     };
     const unsigned long long pol = evict_first_policy();
     const double kk = (double)(ctrl->k_base + it);
-    const double wk = (kk + 1.0) / (kk + 2.0);
-    const double wa = 1.0 / (kk + 2.0);
-    const double step = PRIMAL ? ctrl->tau : ctrl->sigma;
-    const double rho = a.rho;
+    const VT wk = (VT)((kk + 1.0) / (kk + 2.0));
+    const VT wa = (VT)(1.0 / (kk + 2.0));
+    const VT step = (VT)(PRIMAL ? ctrl->tau : ctrl->sigma);
+    const VT rho = (VT)a.rho;
     const int lane = threadIdx.x & 31;
     const int rl = lane % C, sub = lane / C;  // row within the slice, lane group of the row
     const int wpc = blockDim.x >> 5;
@@ -589,20 +593,20 @@ __global__ void __launch_bounds__(1024) k_iter_sell(IterArgs<VT, GT> a, int it) 
         const bool lead = valid && sub == 0;
         const long long p0 = ld_stream((const long long*)a.soff + sl, pol);
         const long long p1 = ld_stream((const long long*)a.soff + sl + 1, pol);
-        const double zr = lead ? a.z[row] : 0.0;
-        const double cst = lead ? a.cost[row] : 0.0;
-        const double zan = lead ? a.za[row] : 0.0;
-        double lo, hi = 0.0;
+        const VT zr = lead ? a.z[row] : (VT)0;
+        const VT cst = lead ? a.cost[row] : (VT)0;
+        const VT zan = lead ? a.za[row] : (VT)0;
+        VT lo, hi = (VT)0;
         if (PRIMAL) {
-            lo = lead ? a.lo[row] : 0.0;
-            hi = lead ? a.hi[row] : 0.0;
+            lo = lead ? a.lo[row] : (VT)0;
+            hi = lead ? a.hi[row] : (VT)0;
         } else {
-            lo = (lead && !a.is_eq[row]) ? (a.ylb ? a.ylb[row] : 0.0) : -INFINITY;
+            lo = (lead && !a.is_eq[row]) ? (a.ylb ? a.ylb[row] : (VT)0) : (VT)(-INFINITY);
         }
         const int nq = (int)((p1 - p0) / (C * W));
         const VT* vp = a.val + p0 + rl * W;
         const int* ip = a.idx + p0 + rl * W;
-        double s_0 = 0.0, s_1 = 0.0;
+        VT s_0 = (VT)0, s_1 = (VT)0;
         // chunk q of this row at vp + q C W; lane group `sub` takes q = sub, sub + LPR, ...
         int q = sub;
         for (; q + LPR < nq; q += 2 * LPR) {
@@ -620,8 +624,8 @@ __global__ void __launch_bounds__(1024) k_iter_sell(IterArgs<VT, GT> a, int it) 
             }
 #pragma unroll
             for (int e = 0; e < W; ++e) {
-                s_0 += (double)v0[e] * (double)g0[e];
-                s_1 += (double)v1[e] * (double)g1[e];
+                s_0 += v0[e] * (VT)g0[e];
+                s_1 += v1[e] * (VT)g1[e];
             }
         }
         if (q < nq) {
@@ -630,29 +634,30 @@ __global__ void __launch_bounds__(1024) k_iter_sell(IterArgs<VT, GT> a, int it) 
             ld_stream_w<W>(vp + (int64_t)q * C * W, v0, pol);
             ld_stream_w<W>(ip + (int64_t)q * C * W, c0, pol);
 #pragma unroll
-            for (int e = 0; e < W; ++e) s_0 += (double)v0[e] * (double)gat(c0[e]);
+            for (int e = 0; e < W; ++e) s_0 += v0[e] * (VT)gat(c0[e]);
         }
-        double s = s_0 + s_1;
+        VT s = s_0 + s_1;
 #pragma unroll
         for (int o = C; o < 32; o <<= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
         if (!lead) continue;
-        double zt;
+        VT zt;
         if (PRIMAL) {
             zt = clampT(zr - step * (cst + s), lo, hi);
-            a.zh[row] = (VT)(2.0 * zt - zr);
+            a.zh[row] = (VT)2 * zt - zr;
         } else {
             zt = zr + step * (s - cst);
             if (zt < lo) zt = lo;  // -inf on equality rows; NaN stays NaN
         }
-        a.z[row] = wk * ((1.0 + rho) * zt - rho * zr) + wa * zan;
+        a.z[row] = wk * (((VT)1 + rho) * zt - rho * zr) + wa * zan;
         if (MODE != M_PLAIN) {
-            const double d = zr - zt;
+            const double d = (double)zr - (double)zt;
             acc_r += d * d;
         }
         if (MODE == M_CHECK) {
             a.zt[row] = zt;
-            if (a.zd) a.zd[row] = (!PRIMAL && lo != -INFINITY) ? fmax(zt - zr, 0.0) : zt - zr;
-            const double e = zt - zan;
+            const double dz = (double)zt - (double)zr;
+            if (a.zd) a.zd[row] = (!PRIMAL && lo != (VT)(-INFINITY)) ? fmax(dz, 0.0) : dz;
+            const double e = (double)zt - (double)zan;
             acc_d += e * e;
         }
     }
@@ -805,10 +810,10 @@ struct KktMap {
 
 // rows: primal residual, b.y, the objective-error sum |y| viol; with xd / yd (the
 // displacement T(z) - z), A xd for the primal ray and the row terms of the dual ray
-template <int L>
+template <int L, typename ZT>
 __global__ void __launch_bounds__(TB) k_kkt_rows(int m, const int32_t* __restrict__ ptr, const int32_t* __restrict__ idx,
-                                                 const double* __restrict__ v64, const double* __restrict__ xt,
-                                                 const double* __restrict__ yt, const double* __restrict__ b,
+                                                 const double* __restrict__ v64, const ZT* __restrict__ xt,
+                                                 const ZT* __restrict__ yt, const double* __restrict__ b,
                                                  const uint8_t* __restrict__ is_eq, const double* __restrict__ dr,
                                                  KktMap map, const double* __restrict__ xd,
                                                  const double* __restrict__ yd, Ctrl* ctrl) {
@@ -824,7 +829,7 @@ __global__ void __launch_bounds__(TB) k_kkt_rows(int m, const int32_t* __restric
         double s = 0.0, sd = 0.0;
         if (valid)
             for (int k = ptr[r] + sub; k < ptr[r + 1]; k += L) {
-                s += v64[k] * xt[idx[k]];
+                s += v64[k] * (double)xt[idx[k]];
                 if (rays) sd += v64[k] * xd[idx[k]];
             }
 #pragma unroll
@@ -838,7 +843,7 @@ __global__ void __launch_bounds__(TB) k_kkt_rows(int m, const int32_t* __restric
             double rp = ax - b[r];
             if (!eq) rp = fmax(rp, 0.0);
             p2 += rp * rp;
-            const double yv = (map.ybar ? map.ybar[r] : 0.0) + ds * (dr[r] * yt[r]);
+            const double yv = (map.ybar ? map.ybar[r] : 0.0) + ds * (dr[r] * (double)yt[r]);
             by += b[r] * yv;
             est += fabs(yv) * fabs(rp);
             if (rays) {
@@ -864,10 +869,10 @@ __global__ void __launch_bounds__(TB) k_kkt_rows(int m, const int32_t* __restric
 // columns: reduced cost g = c + A^T y, bound multipliers lambda, dual residual, c.x and the bound terms
 // columns: reduced cost g = c + A^T y, bound multipliers lambda, dual residual, c.x and the bound
 // terms; with xd / yd, the column terms of the primal ray and A^T yd for the dual ray
-template <int L>
+template <int L, typename ZT>
 __global__ void __launch_bounds__(TB) k_kkt_cols(int n, const int32_t* __restrict__ ptr, const int32_t* __restrict__ idx,
-                                                 const double* __restrict__ v64, const double* __restrict__ yt,
-                                                 const double* __restrict__ xt, const double* __restrict__ c,
+                                                 const double* __restrict__ v64, const ZT* __restrict__ yt,
+                                                 const ZT* __restrict__ xt, const double* __restrict__ c,
                                                  const double* __restrict__ lb, const double* __restrict__ ub,
                                                  const double* __restrict__ dc, KktMap map,
                                                  const double* __restrict__ xd, const double* __restrict__ yd,
@@ -884,7 +889,7 @@ __global__ void __launch_bounds__(TB) k_kkt_cols(int n, const int32_t* __restric
         double s = 0.0, sd = 0.0;
         if (valid)
             for (int k = ptr[j] + sub; k < ptr[j + 1]; k += L) {
-                s += v64[k] * yt[idx[k]];
+                s += v64[k] * (double)yt[idx[k]];
                 if (rays) sd += v64[k] * yd[idx[k]];
             }
 #pragma unroll
@@ -898,7 +903,7 @@ __global__ void __launch_bounds__(TB) k_kkt_cols(int n, const int32_t* __restric
             double lam = (fl && fu) ? g : (fl ? fmax(g, 0.0) : (fu ? fmin(g, 0.0) : 0.0));
             double rd = g - lam;
             d2 += rd * rd;
-            double x = (map.xbar ? map.xbar[j] : 0.0) + ps * (dc[j] * xt[j]);
+            double x = (map.xbar ? map.xbar[j] : 0.0) + ps * (dc[j] * (double)xt[j]);
             pc += c[j] * x;
             if (lam > 0.0) lam_t += lam * lb[j];
             else if (lam < 0.0) lam_t += lam * ub[j];
@@ -1003,26 +1008,24 @@ __global__ void k_control(Ctrl* c) {
     for (int i = 0; i < A_COUNT; ++i) a[i] = 0.0;
 }
 
-// z <- z_anchor <- T(z) at a restart (and the FP32 gather copy of y)
-__global__ void k_restart(int m, int n, const Ctrl* __restrict__ c, double* x, double* xa, const double* __restrict__ xt,
-                          double* y, double* ya, const double* __restrict__ yt, float* yg32) {
+// z <- z_anchor <- T(z) at a restart
+template <typename ZT>
+__global__ void k_restart(int m, int n, const Ctrl* __restrict__ c, ZT* x, ZT* xa, const ZT* __restrict__ xt, ZT* y,
+                          ZT* ya, const ZT* __restrict__ yt) {
     if (c->done || !c->restart) return;
     int tid = blockIdx.x * blockDim.x + threadIdx.x, st = gridDim.x * blockDim.x;
-    for (int j = tid; j < n; j += st) { double v = xt[j]; x[j] = v; xa[j] = v; }
-    for (int i = tid; i < m; i += st) {
-        double v = yt[i];
-        y[i] = v; ya[i] = v;
-        if (yg32) yg32[i] = (float)v;
-    }
+    for (int j = tid; j < n; j += st) { ZT v = xt[j]; x[j] = v; xa[j] = v; }
+    for (int i = tid; i < m; i += st) { ZT v = yt[i]; y[i] = v; ya[i] = v; }
 }
 
 // unscale T(z) into FP64 outputs of the original LP: x = xbar + dc * xt, y = ybar + dr * yt
-__global__ void k_unscale(int m, int n, const double* __restrict__ xt, const double* __restrict__ yt,
+template <typename ZT>
+__global__ void k_unscale(int m, int n, const ZT* __restrict__ xt, const ZT* __restrict__ yt,
                           const double* __restrict__ dr, const double* __restrict__ dc, const double* __restrict__ xbar,
                           const double* __restrict__ ybar, double* __restrict__ xo, double* __restrict__ yo) {
     int tid = blockIdx.x * blockDim.x + threadIdx.x, st = gridDim.x * blockDim.x;
-    for (int j = tid; j < n; j += st) xo[j] = (xbar ? xbar[j] : 0.0) + dc[j] * xt[j];
-    for (int i = tid; i < m; i += st) yo[i] = (ybar ? ybar[i] : 0.0) + dr[i] * yt[i];
+    for (int j = tid; j < n; j += st) xo[j] = (xbar ? xbar[j] : 0.0) + dc[j] * (double)xt[j];
+    for (int i = tid; i < m; i += st) yo[i] = (ybar ? ybar[i] : 0.0) + dr[i] * (double)yt[i];
 }
 
 // ------------------------------------------------------------------ FP64 re-centring (iterative refinement)
@@ -1035,33 +1038,40 @@ __global__ void k_unscale(int m, int n, const double* __restrict__ xt, const dou
 // and xh only ever act on the (small) correction: the residual is exact to FP64
 // after every restart.  The three kernels return at once unless the control
 // kernel has just decided to restart.
+template <typename ZT>
 __global__ void k_rc_update(int m, int n, const Ctrl* __restrict__ c, const double* __restrict__ dr,
-                            const double* __restrict__ dc, double* xbar, double* ybar, double* x, double* xa,
-                            double* xt, double* y, double* ya, double* yt) {
+                            const double* __restrict__ dc, double* xbar, double* ybar, ZT* x, ZT* xa, ZT* xt, ZT* y,
+                            ZT* ya, ZT* yt) {
     if (c->done || !c->restart) return;
     int tid = blockIdx.x * blockDim.x + threadIdx.x, st = gridDim.x * blockDim.x;
     for (int j = tid; j < n; j += st) {
-        xbar[j] += dc[j] * xt[j];
-        x[j] = 0.0; xa[j] = 0.0; xt[j] = 0.0;
+        xbar[j] += dc[j] * (double)xt[j];
+        x[j] = (ZT)0; xa[j] = (ZT)0; xt[j] = (ZT)0;
     }
     for (int i = tid; i < m; i += st) {
-        ybar[i] += dr[i] * yt[i];
-        y[i] = 0.0; ya[i] = 0.0; yt[i] = 0.0;
+        ybar[i] += dr[i] * (double)yt[i];
+        y[i] = (ZT)0; ya[i] = (ZT)0; yt[i] = (ZT)0;
     }
 }
 
+// The shifted problem in FP64 (bs, ylb_s) and, for the mixed engine, its FP32 copy.
 __global__ void k_rc_rows(int m, const Ctrl* __restrict__ c, const int32_t* __restrict__ ptr,
                           const int32_t* __restrict__ idx, const double* __restrict__ vals,
                           const double* __restrict__ xbar, const double* __restrict__ ybar,
                           const double* __restrict__ b, const double* __restrict__ dr, double* axbar, double* bs,
-                          double* ylb_s) {
+                          double* ylb_s, float* bs32, float* ylb32) {
     if (c->done || !c->restart) return;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
         double s = 0.0;
         for (int k = ptr[i]; k < ptr[i + 1]; ++k) s += vals[k] * xbar[idx[k]];
         axbar[i] = s;
-        bs[i] = dr[i] * (b[i] - s);
-        ylb_s[i] = -ybar[i] / dr[i];
+        const double bi = dr[i] * (b[i] - s), li = -ybar[i] / dr[i];
+        bs[i] = bi;
+        ylb_s[i] = li;
+        if (bs32) {
+            bs32[i] = (float)bi;
+            ylb32[i] = (float)li;
+        }
     }
 }
 
@@ -1069,15 +1079,22 @@ __global__ void k_rc_cols(int n, const Ctrl* __restrict__ c, const int32_t* __re
                           const int32_t* __restrict__ idx, const double* __restrict__ vals,
                           const double* __restrict__ xbar, const double* __restrict__ ybar,
                           const double* __restrict__ cost, const double* __restrict__ lb, const double* __restrict__ ub,
-                          const double* __restrict__ dc, double* atybar, double* cs, double* ls, double* us) {
+                          const double* __restrict__ dc, double* atybar, double* cs, double* ls, double* us, float* cs32,
+                          float* ls32, float* us32) {
     if (c->done || !c->restart) return;
     for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
         double s = 0.0;
         for (int k = ptr[j]; k < ptr[j + 1]; ++k) s += vals[k] * ybar[idx[k]];
         atybar[j] = s;
-        cs[j] = dc[j] * (cost[j] + s);
-        ls[j] = (lb[j] - xbar[j]) / dc[j];
-        us[j] = (ub[j] - xbar[j]) / dc[j];
+        const double cj = dc[j] * (cost[j] + s), lj = (lb[j] - xbar[j]) / dc[j], uj = (ub[j] - xbar[j]) / dc[j];
+        cs[j] = cj;
+        ls[j] = lj;
+        us[j] = uj;
+        if (cs32) {
+            cs32[j] = (float)cj;
+            ls32[j] = (float)lj;
+            us32[j] = (float)uj;
+        }
     }
 }
 
@@ -1110,12 +1127,15 @@ void launch_iter(int mode, int L, int R, unsigned grid, int tb, cudaStream_t s, 
     else launch_iter_LR<VT, GT, 1, M_PLAIN, PRIMAL>(L, grid, tb, s, a, it);
 }
 
+template <typename MT>
 void launch_kkt(int Lr, int Lc, unsigned gr, unsigned gc, cudaStream_t s, const DevLP& lp, HalpernWork* w,
                 const KktMap& map, Ctrl* ctrl) {
     const double* xd = w->rays ? w->xd.p : nullptr;
     const double* yd = w->rays ? w->yd.p : nullptr;
-#define KR(LL) k_kkt_rows<LL><<<gr, TB, 0, s>>>(lp.m, lp.rowptr.p, lp.colidx.p, w->sv64.p, w->xt.p, w->yt.p, lp.b.p, lp.is_eq.p, w->dr.p, map, xd, yd, ctrl)
-#define KC(LL) k_kkt_cols<LL><<<gc, TB, 0, s>>>(lp.n, lp.t_rowptr.p, lp.t_colidx.p, w->stv64.p, w->yt.p, w->xt.p, lp.c.p, lp.lb.p, lp.ub.p, w->dc.p, map, xd, yd, ctrl)
+    const MT* xt = (const MT*)w->xt.p;
+    const MT* yt = (const MT*)w->yt.p;
+#define KR(LL) k_kkt_rows<LL, MT><<<gr, TB, 0, s>>>(lp.m, lp.rowptr.p, lp.colidx.p, w->sv64.p, xt, yt, lp.b.p, lp.is_eq.p, w->dr.p, map, xd, yd, ctrl)
+#define KC(LL) k_kkt_cols<LL, MT><<<gc, TB, 0, s>>>(lp.n, lp.t_rowptr.p, lp.t_colidx.p, w->stv64.p, yt, xt, lp.c.p, lp.lb.p, lp.ub.p, w->dc.p, map, xd, yd, ctrl)
     switch (Lr) { case 1: KR(1); break; case 2: KR(2); break; case 4: KR(4); break; case 8: KR(8); break; case 16: KR(16); break; default: KR(32); }
     switch (Lc) { case 1: KC(1); break; case 2: KC(2); break; case 4: KC(4); break; case 8: KC(8); break; case 16: KC(16); break; default: KC(32); }
 #undef KR
@@ -1147,7 +1167,8 @@ int prepare_scaling(Ctx* ctx, HalpernWork* w, int ruiz_iters, bool need32) {
                                    need32 ? w->stv32.p : nullptr);
     unsigned gmn = grid_for(std::max(m, n), TB, ctx->sm_count);
     k_scale_vecs<<<gmn, TB, 0, s>>>(m, n, L.b.p, L.c.p, L.lb.p, L.ub.p, w->dr.p, w->dc.p, w->b64.p, w->c64.p, w->l64.p,
-                                    w->u64.p, nullptr, nullptr, nullptr, nullptr);
+                                    w->u64.p, need32 ? w->b32.p : nullptr, need32 ? w->c32.p : nullptr,
+                                    need32 ? w->l32.p : nullptr, need32 ? w->u32.p : nullptr);
     B2P_LAUNCH(ctx);
     ctx->launches += 4 * ruiz_iters + 7;
     return B2P_OK;
@@ -1386,6 +1407,11 @@ struct Ops<double> {
     static const double* stv(HalpernWork* w) { return w->stv64.p; }
     static double* xh(HalpernWork* w) { return w->xh64.p; }
     static DBuf<double>& sell(Sell& S) { return S.v64; }
+    static const double* c(HalpernWork* w) { return w->c64.p; }
+    static const double* l(HalpernWork* w) { return w->l64.p; }
+    static const double* u(HalpernWork* w) { return w->u64.p; }
+    static const double* b(HalpernWork* w) { return w->b64.p; }
+    static const double* ylb(HalpernWork* w) { return w->ylb_s.p; }
 };
 template <>
 struct Ops<float> {
@@ -1393,16 +1419,24 @@ struct Ops<float> {
     static const float* stv(HalpernWork* w) { return w->stv32.p; }
     static float* xh(HalpernWork* w) { return w->xh32.p; }
     static DBuf<float>& sell(Sell& S) { return S.v32; }
+    static const float* c(HalpernWork* w) { return w->c32.p; }
+    static const float* l(HalpernWork* w) { return w->l32.p; }
+    static const float* u(HalpernWork* w) { return w->u32.p; }
+    static const float* b(HalpernWork* w) { return w->b32.p; }
+    static const float* ylb(HalpernWork* w) { return w->ylb32.p; }
 };
+// the iterates in the engine's precision (the buffers are sized for FP64)
+template <typename MT>
+MT* zbuf(DBuf<double>& d) { return reinterpret_cast<MT*>(d.p); }
 
 // Arguments of the primal kernel (A^T y over A^T, updates x) and of the dual kernel
 // (A xh over A, updates y; with re-centring its sign bound on <= rows is the shifted
 // ylb_s), over the CSR copies or (sell = true) the SELL copies.
 template <typename MT>
-IterArgs<MT, double> primal_args(const DevLP& L, HalpernWork* w, const b2p_params* p, bool sell) {
-    IterArgs<MT, double> a{L.t_rowptr.p, L.t_colidx.p, Ops<MT>::stv(w), w->y.p, w->c64.p, w->l64.p, w->u64.p,
-                           nullptr, nullptr, w->x.p, Ops<MT>::xh(w), w->xa.p, w->xt.p,
-                           w->rays ? w->xd.p : nullptr, w->ctrl.p, L.n, p->reflection, nullptr};
+IterArgs<MT, MT> primal_args(const DevLP& L, HalpernWork* w, const b2p_params* p, bool sell) {
+    IterArgs<MT, MT> a{L.t_rowptr.p, L.t_colidx.p, Ops<MT>::stv(w), zbuf<MT>(w->y), Ops<MT>::c(w), Ops<MT>::l(w),
+                       Ops<MT>::u(w), nullptr, nullptr, zbuf<MT>(w->x), Ops<MT>::xh(w), zbuf<MT>(w->xa),
+                       zbuf<MT>(w->xt), w->rays ? w->xd.p : nullptr, w->ctrl.p, L.n, p->reflection, nullptr};
     if (sell) {
         a.ptr = nullptr;
         a.idx = w->sc->idx.p;
@@ -1415,9 +1449,9 @@ IterArgs<MT, double> primal_args(const DevLP& L, HalpernWork* w, const b2p_param
 }
 template <typename MT>
 IterArgs<MT, MT> dual_args(const DevLP& L, HalpernWork* w, const b2p_params* p, bool sell) {
-    IterArgs<MT, MT> a{L.rowptr.p, L.colidx.p, Ops<MT>::sv(w), Ops<MT>::xh(w), w->b64.p, nullptr, nullptr, L.is_eq.p,
-                       w->recenter ? w->ylb_s.p : nullptr, w->y.p, nullptr, w->ya.p, w->yt.p,
-                       w->rays ? w->yd.p : nullptr, w->ctrl.p, L.m, p->reflection, nullptr};
+    IterArgs<MT, MT> a{L.rowptr.p, L.colidx.p, Ops<MT>::sv(w), Ops<MT>::xh(w), Ops<MT>::b(w), nullptr, nullptr,
+                       L.is_eq.p, w->recenter ? Ops<MT>::ylb(w) : nullptr, zbuf<MT>(w->y), nullptr, zbuf<MT>(w->ya),
+                       zbuf<MT>(w->yt), w->rays ? w->yd.p : nullptr, w->ctrl.p, L.m, p->reflection, nullptr};
     if (sell) {
         a.ptr = nullptr;
         a.idx = w->sr->idx.p;
@@ -1502,15 +1536,15 @@ int sell_win_per_sm(int W, int tb, size_t smem) {
     return per;
 }
 
-// Windows of one side for shape `k` of kWinShapes (primal gathers y: FP64; dual gathers xh: MT).
+// Windows of one side for shape `k` of kWinShapes (primal gathers y, dual gathers xh; both MT).
 template <typename MT>
 int side_windows(Ctx* ctx, HalpernWork* w, bool primal, int k) {
     const DevLP& L = w->ilp;
     const int tb = kWinShapes[k][0];
     const size_t smem = kWinShapes[k][1];
     if (primal)
-        return build_windows(ctx, w->wc, L.n, L.t_rowptr.p, L.t_colidx.p, L.m, tb, smem, sizeof(double),
-                             sell_win_per_sm<MT, double, true>(w->sc_all[0].W, tb, smem));
+        return build_windows(ctx, w->wc, L.n, L.t_rowptr.p, L.t_colidx.p, L.m, tb, smem, sizeof(MT),
+                             sell_win_per_sm<MT, MT, true>(w->sc_all[0].W, tb, smem));
     return build_windows(ctx, w->wr, L.m, L.rowptr.p, L.colidx.p, L.n, tb, smem, sizeof(MT),
                          sell_win_per_sm<MT, MT, false>(w->sr_all[0].W, tb, smem));
 }
@@ -1622,14 +1656,14 @@ int autotune_shapes(Ctx* ctx, HalpernWork* w, const b2p_params* p) {
                 win.smem = 0;
                 g = iter_grid(rows, Lc, R, tb, ctx->sm_count);
             }
-            const IterArgs<MT, double> pa = primal_args<MT>(L, w, p, kind != 0);
+            const IterArgs<MT, MT> pa = primal_args<MT>(L, w, p, kind != 0);
             const IterArgs<MT, MT> da = dual_args<MT>(L, w, p, kind != 0);
             float tot = 0.f;
             for (int rep = 0; rep < 4; ++rep) {
                 cudaEventRecord(e0, s);
-                if (kind != 0 && primal) launch_sell<MT, double, true>(M_PLAIN, **cur, g, tb, smem, s, pa, rep);
+                if (kind != 0 && primal) launch_sell<MT, MT, true>(M_PLAIN, **cur, g, tb, smem, s, pa, rep);
                 else if (kind != 0) launch_sell<MT, MT, false>(M_PLAIN, **cur, g, tb, smem, s, da, rep);
-                else if (primal) launch_iter<MT, double, true>(M_PLAIN, Lc, R, g, tb, s, pa, rep);
+                else if (primal) launch_iter<MT, MT, true>(M_PLAIN, Lc, R, g, tb, s, pa, rep);
                 else launch_iter<MT, MT, false>(M_PLAIN, Lc, R, g, tb, s, da, rep);
                 cudaEventRecord(e1, s);
                 B2P_LAUNCH(ctx);
@@ -1692,6 +1726,7 @@ int run_chunks(Ctx* ctx, HalpernWork* w, const b2p_params* p, double time_limit_
     DevLP& L = w->ilp;
     cudaStream_t s = ctx->stream;
     const int m = L.m, n = L.n, K = p->check_every;
+    const bool mixed = sizeof(MT) == 4;
     const int Lr = w->Lr, Lc = w->Lc, Rr = w->Rr, Rc = w->Rc, Tr = w->Tr, Tc = w->Tc;
     // R = 1 grids serve the two reduction iterations; the KKT kernels use 256-thread grids
     unsigned gr = iter_grid(m, Lr, 1, Tr, ctx->sm_count), gc = iter_grid(n, Lc, 1, Tc, ctx->sm_count);
@@ -1701,35 +1736,41 @@ int run_chunks(Ctx* ctx, HalpernWork* w, const b2p_params* p, double time_limit_
     const int Lkr = pick_lanes(L.mean_row_len, 0), Lkc = pick_lanes(L.mean_col_len, 0);
     unsigned gkr = iter_grid(m, Lkr, 1, TB, ctx->sm_count), gkc = iter_grid(n, Lkc, 1, TB, ctx->sm_count);
     Ctrl* ctrl = w->ctrl.p;
-    const IterArgs<MT, double> pa = primal_args<MT>(L, w, p, w->sell_c);
+    const IterArgs<MT, MT> pa = primal_args<MT>(L, w, p, w->sell_c);
     const IterArgs<MT, MT> da = dual_args<MT>(L, w, p, w->sell_r);
     auto chunk = [&]() {
         for (int i = 0; i < K; ++i) {
             int mode = (i == 0) ? M_FIRST : (i == K - 1 ? M_CHECK : M_PLAIN);
-            if (w->sell_c) launch_sell<MT, double, true>(mode, *w->sc, gcS, Tc, w->wc.smem, s, pa, i);
-            else if (mode == M_PLAIN) launch_iter<MT, double, true>(mode, Lc, Rc, gcR, Tc, s, pa, i);
-            else launch_iter<MT, double, true>(mode, Lc, 1, gc, Tc, s, pa, i);
+            if (w->sell_c) launch_sell<MT, MT, true>(mode, *w->sc, gcS, Tc, w->wc.smem, s, pa, i);
+            else if (mode == M_PLAIN) launch_iter<MT, MT, true>(mode, Lc, Rc, gcR, Tc, s, pa, i);
+            else launch_iter<MT, MT, true>(mode, Lc, 1, gc, Tc, s, pa, i);
             if (w->sell_r) launch_sell<MT, MT, false>(mode, *w->sr, grS, Tr, w->wr.smem, s, da, i);
             else if (mode == M_PLAIN) launch_iter<MT, MT, false>(mode, Lr, Rr, grR, Tr, s, da, i);
             else launch_iter<MT, MT, false>(mode, Lr, 1, gr, Tr, s, da, i);
         }
         const KktMap map = w->recenter ? KktMap{w->xbar.p, w->ybar.p, w->axbar.p, w->atybar.p}
                                        : KktMap{nullptr, nullptr, nullptr, nullptr};
-        launch_kkt(Lkr, Lkc, gkr, gkc, s, L, w, map, ctrl);
+        launch_kkt<MT>(Lkr, Lkc, gkr, gkc, s, L, w, map, ctrl);
         k_control<<<1, 1, 0, s>>>(ctrl);
         const unsigned gv = grid_for(std::max(m, n), TB, ctx->sm_count, 8);
         if (w->recenter) {
-            k_rc_update<<<gv, TB, 0, s>>>(m, n, ctrl, w->dr.p, w->dc.p, w->xbar.p, w->ybar.p, w->x.p, w->xa.p, w->xt.p,
-                                          w->y.p, w->ya.p, w->yt.p);
+            k_rc_update<MT><<<gv, TB, 0, s>>>(m, n, ctrl, w->dr.p, w->dc.p, w->xbar.p, w->ybar.p, zbuf<MT>(w->x),
+                                              zbuf<MT>(w->xa), zbuf<MT>(w->xt), zbuf<MT>(w->y), zbuf<MT>(w->ya),
+                                              zbuf<MT>(w->yt));
             k_rc_rows<<<grid_for(m, TB, ctx->sm_count, 8), TB, 0, s>>>(m, ctrl, L.rowptr.p, L.colidx.p, L.vals.p,
                                                                       w->xbar.p, w->ybar.p, L.b.p, w->dr.p,
-                                                                      w->axbar.p, w->b64.p, w->ylb_s.p);
+                                                                      w->axbar.p, w->b64.p, w->ylb_s.p,
+                                                                      mixed ? w->b32.p : nullptr,
+                                                                      mixed ? w->ylb32.p : nullptr);
             k_rc_cols<<<grid_for(n, TB, ctx->sm_count, 8), TB, 0, s>>>(n, ctrl, L.t_rowptr.p, L.t_colidx.p, L.t_vals.p,
                                                                       w->xbar.p, w->ybar.p, L.c.p, L.lb.p, L.ub.p,
                                                                       w->dc.p, w->atybar.p, w->c64.p, w->l64.p,
-                                                                      w->u64.p);
+                                                                      w->u64.p, mixed ? w->c32.p : nullptr,
+                                                                      mixed ? w->l32.p : nullptr,
+                                                                      mixed ? w->u32.p : nullptr);
         } else {
-            k_restart<<<gv, TB, 0, s>>>(m, n, ctrl, w->x.p, w->xa.p, w->xt.p, w->y.p, w->ya.p, w->yt.p, nullptr);
+            k_restart<MT><<<gv, TB, 0, s>>>(m, n, ctrl, zbuf<MT>(w->x), zbuf<MT>(w->xa), zbuf<MT>(w->xt),
+                                            zbuf<MT>(w->y), zbuf<MT>(w->ya), zbuf<MT>(w->yt));
         }
     };
     cudaGraph_t graph = nullptr;
@@ -1811,6 +1852,10 @@ int solve_T(Ctx* ctx, HalpernWork* w, const b2p_params* p, const double* x0, con
             B2P_CUDA(ctx, b->reserve(m));
             B2P_CUDA(ctx, cudaMemsetAsync(b->p, 0, sizeof(double) * m, s));
         }
+        if (mixed) {
+            B2P_CUDA(ctx, w->ylb32.reserve(m));
+            B2P_CUDA(ctx, cudaMemsetAsync(w->ylb32.p, 0, sizeof(float) * m, s));
+        }
     }
     w->rays = p->eps_infeasible > 0.0;
     if (w->rays) {
@@ -1876,9 +1921,9 @@ int solve_T(Ctx* ctx, HalpernWork* w, const b2p_params* p, const double* x0, con
         ctx->launches += 1;
         y0d = w->pu.p;
     }
-    k_init_iterates<<<grid_for(std::max(m, n), TB, ctx->sm_count), TB, 0, s>>>(
-        m, n, w->l64.p, w->u64.p, x0d, y0d, w->dr.p, w->dc.p, L.is_eq.p, nullptr, w->x.p, w->xa.p, w->xt.p, w->y.p, w->ya.p,
-        w->yt.p, nullptr);
+    k_init_iterates<MT><<<grid_for(std::max(m, n), TB, ctx->sm_count), TB, 0, s>>>(
+        m, n, w->l64.p, w->u64.p, x0d, y0d, w->dr.p, w->dc.p, L.is_eq.p, nullptr, zbuf<MT>(w->x), zbuf<MT>(w->xa),
+        zbuf<MT>(w->xt), zbuf<MT>(w->y), zbuf<MT>(w->ya), zbuf<MT>(w->yt));
     B2P_LAUNCH(ctx);
     ctx->launches += 1;
     Ctrl hc;
@@ -1909,9 +1954,9 @@ int solve_T(Ctx* ctx, HalpernWork* w, const b2p_params* p, const double* x0, con
         st = autotune_shapes<MT>(ctx, w, p);  // returns at once when this LP shape is already tuned
         if (st) return st;
         if (before != w->tuned_key && w->tuned_key >= 0) {  // the trial iterations moved the iterates: reset
-            k_init_iterates<<<grid_for(std::max(m, n), TB, ctx->sm_count), TB, 0, s>>>(
-                m, n, w->l64.p, w->u64.p, x0d, y0d, w->dr.p, w->dc.p, L.is_eq.p, nullptr, w->x.p, w->xa.p, w->xt.p, w->y.p,
-                w->ya.p, w->yt.p, nullptr);
+            k_init_iterates<MT><<<grid_for(std::max(m, n), TB, ctx->sm_count), TB, 0, s>>>(
+                m, n, w->l64.p, w->u64.p, x0d, y0d, w->dr.p, w->dc.p, L.is_eq.p, nullptr, zbuf<MT>(w->x),
+                zbuf<MT>(w->xa), zbuf<MT>(w->xt), zbuf<MT>(w->y), zbuf<MT>(w->ya), zbuf<MT>(w->yt));
             B2P_LAUNCH(ctx);
             ctx->launches += 1;
             B2P_CUDA(ctx, cudaMemcpyAsync(w->ctrl.p, &hc, sizeof(Ctrl), cudaMemcpyHostToDevice, s));
@@ -1943,8 +1988,8 @@ int solve_T(Ctx* ctx, HalpernWork* w, const b2p_params* p, const double* x0, con
     r->refinement_rounds_done = w->recenter ? (int)fin.restarts : 0;
     if (x_out || y_out) {
         double t0 = now_ms();
-        k_unscale<<<grid_for(std::max(m, n), TB, ctx->sm_count), TB, 0, s>>>(
-            m, n, w->xt.p, w->yt.p, w->dr.p, w->dc.p, w->recenter ? w->xbar.p : nullptr,
+        k_unscale<MT><<<grid_for(std::max(m, n), TB, ctx->sm_count), TB, 0, s>>>(
+            m, n, zbuf<MT>(w->xt), zbuf<MT>(w->yt), w->dr.p, w->dc.p, w->recenter ? w->xbar.p : nullptr,
             w->recenter ? w->ybar.p : nullptr, w->tmp_n.p, w->tmp_m.p);
         // internal -> original numbering
         k_scatter_perm<double><<<grid_for(n, TB, ctx->sm_count), TB, 0, s>>>(n, w->pc.p, w->tmp_n.p, w->pv.p);
@@ -1978,15 +2023,15 @@ int kernel_timing_T(Ctx* ctx, HalpernWork* w, const b2p_params* p, int reps, dou
     Ctrl open = saved;
     open.done = 0;
     B2P_CUDA(ctx, cudaMemcpyAsync(ctrl, &open, sizeof(Ctrl), cudaMemcpyHostToDevice, s));
-    const IterArgs<MT, double> pa = primal_args<MT>(L, w, p, w->sell_c);
+    const IterArgs<MT, MT> pa = primal_args<MT>(L, w, p, w->sell_c);
     const IterArgs<MT, MT> da = dual_args<MT>(L, w, p, w->sell_r);
     cudaEvent_t e[3];
     for (auto& x : e) B2P_CUDA(ctx, cudaEventCreate(&x));
     double tp = 0, td = 0;
     for (int r = 0; r < reps; ++r) {
         cudaEventRecord(e[0], s);
-        if (w->sell_c) launch_sell<MT, double, true>(M_PLAIN, *w->sc, gc, Tc, w->wc.smem, s, pa, r);
-        else launch_iter<MT, double, true>(M_PLAIN, Lc, Rc, gc, Tc, s, pa, r);
+        if (w->sell_c) launch_sell<MT, MT, true>(M_PLAIN, *w->sc, gc, Tc, w->wc.smem, s, pa, r);
+        else launch_iter<MT, MT, true>(M_PLAIN, Lc, Rc, gc, Tc, s, pa, r);
         cudaEventRecord(e[1], s);
         if (w->sell_r) launch_sell<MT, MT, false>(M_PLAIN, *w->sr, gr, Tr, w->wr.smem, s, da, r);
         else launch_iter<MT, MT, false>(M_PLAIN, Lr, Rr, gr, Tr, s, da, r);
@@ -2010,10 +2055,10 @@ int kernel_timing_T(Ctx* ctx, HalpernWork* w, const b2p_params* p, int reps, dou
     const double vb = sizeof(MT), nnz = (double)L.nnz;
     const double pc_bytes = w->sell_c ? 8.0 * (w->sc->slices + 1) : 4.0 * (n + 1);
     const double pr_bytes = w->sell_r ? 8.0 * (w->sr->slices + 1) : 4.0 * (m + 1);
-    // primal: A^T values+indices, col pointers, gather y (m x 8), x r/w, xa, c, l, u (8 each), xh write
-    *pb = nnz * (vb + 4) + pc_bytes + 8.0 * m + n * (8 * 6 + vb);
-    // dual: A values+indices, row pointers, gather xh (n x vb), y r/w, ya, b (8 each), is_eq (1)
-    *db = nnz * (vb + 4) + pr_bytes + vb * n + m * (8 * 4 + 1);
+    // primal: A^T values+indices, col pointers, gather y, x r/w, xa, c, l, u, xh write (vb bytes each)
+    *pb = nnz * (vb + 4) + pc_bytes + vb * m + n * (vb * 7);
+    // dual: A values+indices, row pointers, gather xh, y r/w, ya, b, dual bound (vb each), is_eq (1)
+    *db = nnz * (vb + 4) + pr_bytes + vb * n + m * (vb * 5 + 1);
     return B2P_OK;
 }
 
@@ -2064,6 +2109,10 @@ int halpern_engine_solve(Ctx* ctx, const b2p_params* p, const double* x0, const 
     for (auto* b : {&w->dc, &w->tmp_n, &w->pv, &w->c64, &w->l64, &w->u64, &w->x, &w->xa, &w->xt})
         B2P_CUDA(ctx, b->reserve(n));
     for (auto* b : {&w->dr, &w->tmp_m, &w->pu, &w->b64, &w->y, &w->ya, &w->yt}) B2P_CUDA(ctx, b->reserve(m));
+    if (p->precision == B2P_FP32) {
+        for (auto* b : {&w->c32, &w->l32, &w->u32}) B2P_CUDA(ctx, b->reserve(n));
+        for (auto* b : {&w->b32, &w->ylb32}) B2P_CUDA(ctx, b->reserve(m));
+    }
     B2P_CUDA(ctx, w->pw.reserve(64));
     B2P_CUDA(ctx, w->sv64.reserve(nnz));
     B2P_CUDA(ctx, w->stv64.reserve(nnz));
