@@ -596,6 +596,17 @@ def run_learned_workload(args):
                 "note": "12 B per nonzero (FP32 value + 16-bit index, both orientations), 24 B per column, 16 B per "
                         "row; bound 'l2': the shared matrix and the instances' vectors stay in L2 / shared memory "
                         "(ncu: DRAM carries dram_frac of these bytes)"}
+    # training on the tensor cores: GEMM FLOPs of all epochs (per sample: layer 1 forward +
+    # weight gradient, layers 2 and 3 forward + weight gradient + input gradient) over the
+    # training time, against the sustained BF16 peak
+    hid, outp = 1024, (fam.n + fam.m + 1 + 7) // 8 * 8
+    flop = (4.0 * fam.N_PARAM * hid + 6.0 * hid * hid + 6.0 * hid * outp) * args.train_count * args.epochs
+    bf16 = peaks.get("bf16_tflops_sustained") or peaks.get("bf16_tflops") or 1400.0
+    fit["train_tflops"] = flop / max(fit["train_s"], 1e-9) / 1e12
+    fit["train_frac_of_bf16_sustained"] = fit["train_tflops"] / bf16
+    fit["train_peak_source"] = ("MEASURED_PEAKS.json (of measured)" if peaks.get("bf16_tflops_sustained")
+                                else "fallback 1400 TFLOP/s sustained BF16 (of fallback)")
+    fit["train_flop"] = flop
     cpu = None
     if rank == 0 and world == 1:
         lp0 = fam.instance(P[0])

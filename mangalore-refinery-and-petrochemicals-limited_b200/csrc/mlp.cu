@@ -49,6 +49,18 @@ struct MlpState {
     DBuf<__nv_bfloat16> Xh, Xt, H1, H1t, H2, H2t, dY, dYt, dZ, dZt;
     DBuf<double> loss;
     DBuf<int> err;
+    // Adam on the device: hyper = {learning rate, 1 - beta1^t, 1 - beta2^t}, t in dstep
+    DBuf<float> hyper;
+    DBuf<long long> dstep;
+    // split-K partial sums of the GEMMs whose output tiles alone would leave most SMs idle
+    DBuf<float> ws;
+    // one training epoch captured as a CUDA graph (for this data-set size and batch)
+    cudaGraphExec_t epoch_exec = nullptr;
+    int epoch_n = 0, epoch_batch = 0;
+    long long epoch_launches = 0;  // kernels one replay launches
+    ~MlpState() {
+        if (epoch_exec) cudaGraphExecDestroy(epoch_exec);
+    }
     // normalisation of inputs and targets: v_norm = (v - mean) / std
     DBuf<float> in_mean, in_std, out_mean, out_std;
     bool has_norm = false;
@@ -152,9 +164,10 @@ constexpr int GTILE_A = GBM * GBK * 2, GTILE_B = GBN * GBK * 2;
 constexpr size_t GEMM_SMEM = 1024 + GSTAGES * (GTILE_A + GTILE_B) + 256;
 
 // C[M,N] = A[M,K] . B[N,K]^T ; A, B through tensor maps; C FP32 row-major, ldc elements.
+// Split-K: CTA z of gridDim.z sums k-blocks [z kbs, (z + 1) kbs) into C + z split_stride.
 __global__ void __launch_bounds__(128, 1)
 k_gemm_tn_bf16(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, float* __restrict__ C,
-               int M, int N, int K, int ldc, int* err) {
+               int M, int N, int K, int ldc, int kbs, size_t split_stride, int* err) {
     extern __shared__ uint8_t smem_raw[];
     uint8_t* base = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);  // SW128 tiles: 1024-aligned
     uint8_t* sA = base;
@@ -165,7 +178,9 @@ k_gemm_tn_bf16(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
     uint32_t* tmem_slot = (uint32_t*)(accum + 1);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int m0 = blockIdx.y * GBM, n0 = blockIdx.x * GBN;
-    const int nkb = (K + GBK - 1) / GBK;
+    const int kb0 = blockIdx.z * kbs;
+    const int nkb = min((K + GBK - 1) / GBK - kb0, kbs);  // k-blocks of this split (>= 1 by construction)
+    C += blockIdx.z * split_stride;
 
     if (warp == 0) {  // TMEM: 128 FP32 columns for the 128 x 128 accumulator
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
@@ -194,8 +209,8 @@ k_gemm_tn_bf16(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
             if (kb >= GSTAGES) ok = mbar_wait(&empty[s], ph ^ 1, err, 1);
             if (!ok) break;
             mbar_expect_tx(&full[s], GTILE_A + GTILE_B);
-            tma_load_2d(sA + s * GTILE_A, &tmA, &full[s], kb * GBK, m0);
-            tma_load_2d(sB + s * GTILE_B, &tmB, &full[s], kb * GBK, n0);
+            tma_load_2d(sA + s * GTILE_A, &tmA, &full[s], (kb0 + kb) * GBK, m0);
+            tma_load_2d(sB + s * GTILE_B, &tmB, &full[s], (kb0 + kb) * GBK, n0);
         }
     } else if (warp == 1 && lane == 0) {  // MMA issuer
         const uint32_t idesc = idesc_bf16(GBM, GBN);
@@ -270,9 +285,24 @@ bool make_map(CUtensorMap* map, const void* ptr, int rows, int cols, int ld, int
               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
-// C[M,N] = A[M,K] B[N,K]^T; all leading dimensions multiples of 8.
+// C = sum of `splits` partial tiles (fixed order: deterministic)
+__global__ void k_splitk_reduce(int M, int N, int ldc, int splits, size_t stride, const float* __restrict__ ws,
+                                float* __restrict__ C) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < (long long)M * N;
+         i += (long long)gridDim.x * blockDim.x) {
+        const size_t o = (size_t)(i / N) * ldc + (size_t)(i % N);
+        float acc = 0.0f;
+        for (int z = 0; z < splits; ++z) acc += ws[z * stride + o];
+        C[o] = acc;
+    }
+}
+
+// C[M,N] = A[M,K] B[N,K]^T; all leading dimensions multiples of 8.  With a workspace, a GEMM
+// whose output tiles would occupy fewer than half of the SMs and whose K spans at least
+// 8 k-blocks is split along K (each split >= 4 k-blocks), the partial tiles summed by
+// k_splitk_reduce.
 int gemm_tn(Ctx* ctx, const __nv_bfloat16* A, int lda, const __nv_bfloat16* B, int ldb, float* C, int ldc, int M, int N,
-            int K, int* err) {
+            int K, int* err, DBuf<float>* ws = nullptr) {
     CUtensorMap ta, tb;
     if (!make_map(&ta, A, M, K, lda, GBM) || !make_map(&tb, B, N, K, ldb, GBN)) {
         ctx->err = "gemm: tensor map rejected (alignment) or driver entry point missing";
@@ -283,10 +313,27 @@ int gemm_tn(Ctx* ctx, const __nv_bfloat16* A, int lda, const __nv_bfloat16* B, i
         B2P_CUDA(ctx, cudaFuncSetAttribute(k_gemm_tn_bf16, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)GEMM_SMEM));
         attr = true;
     }
-    dim3 grid((N + GBN - 1) / GBN, (M + GBM - 1) / GBM);
-    k_gemm_tn_bf16<<<grid, 128, GEMM_SMEM, ctx->stream>>>(ta, tb, C, M, N, K, ldc, err);
-    B2P_LAUNCH(ctx);
+    const int tiles = ((N + GBN - 1) / GBN) * ((M + GBM - 1) / GBM);
+    const int nkb = (K + GBK - 1) / GBK;
+    int splits = 1;
+    if (ws && 2 * tiles <= ctx->sm_count && nkb >= 8) splits = std::max(1, std::min(nkb / 4, ctx->sm_count / tiles));
+    const int kbs = (nkb + splits - 1) / splits;
+    splits = (nkb + kbs - 1) / kbs;  // every split gets at least one k-block
+    const size_t stride = (size_t)M * ldc;
+    float* out = C;
+    if (splits > 1) {
+        B2P_CUDA(ctx, ws->reserve(stride * splits));
+        out = ws->p;
+    }
+    dim3 grid((N + GBN - 1) / GBN, (M + GBM - 1) / GBM, splits);
+    k_gemm_tn_bf16<<<grid, 128, GEMM_SMEM, ctx->stream>>>(ta, tb, out, M, N, K, ldc, kbs, stride, err);
     ctx->launches += 1;
+    if (splits > 1) {
+        k_splitk_reduce<<<grid_for((long long)M * N, 256, ctx->sm_count, 8), 256, 0, ctx->stream>>>(M, N, ldc, splits,
+                                                                                                   stride, ws->p, C);
+        ctx->launches += 1;
+    }
+    B2P_LAUNCH(ctx);
     return B2P_OK;
 }
 
@@ -302,16 +349,44 @@ __device__ __forceinline__ float gelu_grad(float x) {
     return 0.5f * (1.0f + t) + 0.5f * x * (1.0f - t * t) * k * (1.0f + 3.0f * 0.044715f * x * x);
 }
 
+// 32 x 32 tiles of a rows x cols matrix, one tile at a time per CTA of 32 x 8 threads:
+// f(r, c) computes element (r, c) once (with its side effects); the BF16 result goes to
+// out (row-major, ld_out; stores coalesced along c) and, through a shared-memory tile,
+// to outT (its transpose, ld_t; stores coalesced along r).  Either output may be null.
+constexpr int kTileThreadsY = 8;
+template <typename F>
+__device__ __forceinline__ void tile_pass(int rows, int cols, __nv_bfloat16* out, int ld_out, __nv_bfloat16* outT,
+                                          int ld_t, F f) {
+    __shared__ __nv_bfloat16 t[32][34];
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    const int tiles_c = (cols + 31) / 32, tiles = tiles_c * ((rows + 31) / 32);
+    for (int tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+        const int r0 = (tile / tiles_c) * 32, c0 = (tile % tiles_c) * 32;
+#pragma unroll
+        for (int k = 0; k < 32; k += kTileThreadsY) {
+            const int r = r0 + ty + k, c = c0 + tx;
+            if (r < rows && c < cols) {
+                const __nv_bfloat16 v = f(r, c);
+                if (out) out[(size_t)r * ld_out + c] = v;
+                t[ty + k][tx] = v;
+            }
+        }
+        if (!outT) continue;
+        __syncthreads();
+#pragma unroll
+        for (int k = 0; k < 32; k += kTileThreadsY) {
+            const int c = c0 + ty + k, r = r0 + tx;
+            if (r < rows && c < cols) outT[(size_t)c * ld_t + r] = t[tx][ty + k];
+        }
+        __syncthreads();
+    }
+}
+
 // FP32 rows x cols (ld_in) -> BF16 copy (ld_out) and optional BF16 transpose (cols x rows, ld_t)
 __global__ void k_to_bf16(int rows, int cols, const float* __restrict__ in, int ld_in, __nv_bfloat16* out, int ld_out,
                           __nv_bfloat16* outT, int ld_t) {
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < (long long)rows * cols;
-         i += (long long)gridDim.x * blockDim.x) {
-        const int r = (int)(i / cols), c = (int)(i % cols);
-        const __nv_bfloat16 v = __float2bfloat16(in[(size_t)r * ld_in + c]);
-        if (out) out[(size_t)r * ld_out + c] = v;
-        if (outT) outT[(size_t)c * ld_t + r] = v;
-    }
+    tile_pass(rows, cols, out, ld_out, outT, ld_t,
+              [&](int r, int c) { return __float2bfloat16(in[(size_t)r * ld_in + c]); });
 }
 
 // BF16 rows x cols -> BF16 transpose
@@ -329,15 +404,12 @@ __global__ void k_transpose_bf16(int rows, int cols, const __nv_bfloat16* __rest
 __global__ void k_bias_gelu(int rows, int valid, int cols, const float* __restrict__ G, const float* __restrict__ bias,
                             float* __restrict__ Z, __nv_bfloat16* __restrict__ H, __nv_bfloat16* __restrict__ Ht,
                             int ld_t) {
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < (long long)rows * cols;
-         i += (long long)gridDim.x * blockDim.x) {
-        const int r = (int)(i / cols), c = (int)(i % cols);
+    tile_pass(rows, cols, H, cols, Ht, ld_t, [&](int r, int c) {
+        const size_t i = (size_t)r * cols + c;
         const float z = r < valid ? G[i] + bias[c] : 0.0f;
-        const __nv_bfloat16 h = __float2bfloat16(r < valid ? gelu(z) : 0.0f);
         if (Z) Z[i] = z;
-        H[i] = h;
-        if (Ht) Ht[(size_t)c * ld_t + r] = h;
-    }
+        return __float2bfloat16(r < valid ? gelu(z) : 0.0f);
+    });
 }
 
 // Y = G + b3; squared error against T on the valid rows / real columns; dY = 2 (Y - T) / (valid * out)
@@ -347,9 +419,8 @@ __global__ void k_out_loss(int rows, int valid, int out, int outp, const float* 
                            bool want_grad) {
     double part = 0.0;
     const float scale = 2.0f / ((float)valid * (float)out);
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < (long long)rows * outp;
-         i += (long long)gridDim.x * blockDim.x) {
-        const int r = (int)(i / outp), c = (int)(i % outp);
+    tile_pass(rows, outp, want_grad ? dY : nullptr, outp, want_grad ? dYt : nullptr, ld_t, [&](int r, int c) {
+        const size_t i = (size_t)r * outp + c;
         const float y = G[i] + bias[c];
         if (Y) Y[i] = y;
         float g = 0.0f;
@@ -358,12 +429,8 @@ __global__ void k_out_loss(int rows, int valid, int out, int outp, const float* 
             part += (double)d * d;
             g = scale * d;
         }
-        if (want_grad) {
-            const __nv_bfloat16 gb = __float2bfloat16(g);
-            dY[i] = gb;
-            dYt[(size_t)c * ld_t + r] = gb;
-        }
-    }
+        return __float2bfloat16(g);
+    });
     if (loss) {
         part = warp_sum(part);
         if ((threadIdx.x & 31) == 0 && part != 0.0) atomicAdd(loss, part);
@@ -373,14 +440,10 @@ __global__ void k_out_loss(int rows, int valid, int out, int outp, const float* 
 // dZ = G * GELU'(Z) (BF16 + transpose), rows >= valid zeroed
 __global__ void k_gelu_back(int rows, int valid, int cols, const float* __restrict__ G, const float* __restrict__ Z,
                             __nv_bfloat16* __restrict__ dZ, __nv_bfloat16* __restrict__ dZt, int ld_t) {
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < (long long)rows * cols;
-         i += (long long)gridDim.x * blockDim.x) {
-        const int r = (int)(i / cols), c = (int)(i % cols);
-        const float g = r < valid ? G[i] * gelu_grad(Z[i]) : 0.0f;
-        const __nv_bfloat16 v = __float2bfloat16(g);
-        dZ[i] = v;
-        dZt[(size_t)c * ld_t + r] = v;
-    }
+    tile_pass(rows, cols, dZ, cols, dZt, ld_t, [&](int r, int c) {
+        const size_t i = (size_t)r * cols + c;
+        return __float2bfloat16(r < valid ? G[i] * gelu_grad(Z[i]) : 0.0f);
+    });
 }
 
 // db[c] = sum over rows of a BF16 gradient (FP32 accumulation); one thread per column
@@ -392,28 +455,44 @@ __global__ void k_colsum(int rows, int cols, const __nv_bfloat16* __restrict__ D
     }
 }
 
-// Adam on FP32 master weights (rows x cols, ld == cols), then BF16 copy and transpose.
-__global__ void k_adam(long long n, int cols, float* __restrict__ w, const float* __restrict__ g, float* __restrict__ m,
-                       float* __restrict__ v, float lr, float b1t, float b2t, __nv_bfloat16* __restrict__ wh,
+// One Adam update of element i; hyper = {learning rate, 1 - beta1^t, 1 - beta2^t}.
+__device__ __forceinline__ float adam_update(size_t i, float* __restrict__ w, const float* __restrict__ g,
+                                             float* __restrict__ m, float* __restrict__ v, const float* hyper) {
+    const float gi = g[i];
+    const float mi = 0.9f * m[i] + 0.1f * gi;
+    const float vi = 0.999f * v[i] + 0.001f * gi * gi;
+    m[i] = mi;
+    v[i] = vi;
+    const float wi = w[i] - hyper[0] * (mi / hyper[1]) / (sqrtf(vi / hyper[2]) + 1e-8f);
+    w[i] = wi;
+    return wi;
+}
+
+// Adam of a bias vector (n elements).
+__global__ void k_adam_vec(int n, float* __restrict__ w, const float* __restrict__ g, float* __restrict__ m,
+                           float* __restrict__ v, const float* __restrict__ hyper) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) adam_update(i, w, g, m, v, hyper);
+}
+
+// Adam on FP32 master weights (rows x cols, ld == cols) for the first live_rows rows, then
+// their BF16 copy and its transpose (cols x rows, ld_t); hyper null: no update, copies only.
+__global__ void k_adam(int rows, int cols, float* __restrict__ w, const float* __restrict__ g, float* __restrict__ m,
+                       float* __restrict__ v, const float* __restrict__ hyper, __nv_bfloat16* __restrict__ wh,
                        __nv_bfloat16* __restrict__ wt, int ld_t, int live_rows) {
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
-        const int r = (int)(i / cols), c = (int)(i % cols);
-        float wi = w[i];
-        if (r < live_rows) {
-            const float gi = g[i];
-            const float mi = 0.9f * m[i] + 0.1f * gi;
-            const float vi = 0.999f * v[i] + 0.001f * gi * gi;
-            m[i] = mi;
-            v[i] = vi;
-            wi -= lr * (mi / b1t) / (sqrtf(vi / b2t) + 1e-8f);
-            w[i] = wi;
-        }
-        if (wh) {
-            const __nv_bfloat16 h = __float2bfloat16(wi);
-            wh[i] = h;
-            if (wt) wt[(size_t)c * ld_t + r] = h;
-        }
-    }
+    tile_pass(rows, cols, wh, cols, wt, ld_t, [&](int r, int c) {
+        const size_t i = (size_t)r * cols + c;
+        const float wi = (hyper && r < live_rows) ? adam_update(i, w, g, m, v, hyper) : w[i];
+        return __float2bfloat16(wi);
+    });
+}
+
+// Start of an Adam step on the device: t += 1, the bias corrections of step t, and the
+// learning rate when lr >= 0 (a negative lr keeps the rate already in hyper[0]).
+__global__ void k_adam_begin(long long* __restrict__ step, float* __restrict__ hyper, float lr) {
+    const long long t = ++*step;
+    hyper[1] = 1.0f - powf(0.9f, (float)t);
+    hyper[2] = 1.0f - powf(0.999f, (float)t);
+    if (lr >= 0.0f) hyper[0] = lr;
 }
 
 // deterministic init: U(-a, a), a = 1/sqrt(fan_in) (the default of a linear layer)
@@ -507,6 +586,11 @@ __global__ void k_denorm_warm(int valid, int outp, int n, int m, const float* __
 
 // ---------------------------------------------------------------- MLP host side
 unsigned ew_grid(Ctx* ctx, long long n) { return grid_for(n, 256, ctx->sm_count, 8); }
+// grid of a tile_pass kernel over a rows x cols matrix (blocks of 32 x 8 threads)
+unsigned tile_grid(Ctx* ctx, long long rows, long long cols) {
+    return grid_for(((rows + 31) / 32) * ((cols + 31) / 32) * 256, 256, ctx->sm_count, 8);
+}
+const dim3 kTileBlock(32, kTileThreadsY);
 
 int check_err(Ctx* ctx, MlpState* s) {
     int e = 0;
@@ -540,11 +624,11 @@ int forward(Ctx* ctx, MlpState* s, int rows, int valid, bool keep) {
     const int in = s->in, h = s->hid, op = s->outp;
     cudaStream_t st = ctx->stream;
     int r;
-    if ((r = gemm_tn(ctx, s->Xh.p, in, s->W1h.p, in, s->G.p, h, rows, h, in, s->err.p))) return r;
-    k_bias_gelu<<<ew_grid(ctx, (long long)rows * h), 256, 0, st>>>(rows, valid, h, s->G.p, s->b1.p, s->Z1.p, s->H1.p,
+    if ((r = gemm_tn(ctx, s->Xh.p, in, s->W1h.p, in, s->G.p, h, rows, h, in, s->err.p, &s->ws))) return r;
+    k_bias_gelu<<<tile_grid(ctx, rows, h), kTileBlock, 0, st>>>(rows, valid, h, s->G.p, s->b1.p, s->Z1.p, s->H1.p,
                                                                     keep ? s->H1t.p : nullptr, rows);
-    if ((r = gemm_tn(ctx, s->H1.p, h, s->W2h.p, h, s->G.p, h, rows, h, h, s->err.p))) return r;
-    k_bias_gelu<<<ew_grid(ctx, (long long)rows * h), 256, 0, st>>>(rows, valid, h, s->G.p, s->b2.p, s->Z2.p, s->H2.p,
+    if ((r = gemm_tn(ctx, s->H1.p, h, s->W2h.p, h, s->G.p, h, rows, h, h, s->err.p, &s->ws))) return r;
+    k_bias_gelu<<<tile_grid(ctx, rows, h), kTileBlock, 0, st>>>(rows, valid, h, s->G.p, s->b2.p, s->Z2.p, s->H2.p,
                                                                     keep ? s->H2t.p : nullptr, rows);
     if ((r = gemm_tn(ctx, s->H2.p, h, s->W3h.p, h, s->G.p, op, rows, op, h, s->err.p))) return r;
     B2P_LAUNCH(ctx);
@@ -557,45 +641,47 @@ int backward(Ctx* ctx, MlpState* s, int rows, int valid) {
     const int in = s->in, h = s->hid, op = s->outp, out = s->out;
     cudaStream_t st = ctx->stream;
     int r;
-    k_out_loss<<<ew_grid(ctx, (long long)rows * op), 256, 0, st>>>(rows, valid, out, op, s->G.p, s->b3.p, s->Tf.p,
+    k_out_loss<<<tile_grid(ctx, rows, op), kTileBlock, 0, st>>>(rows, valid, out, op, s->G.p, s->b3.p, s->Tf.p,
                                                                     s->Y.p, s->dY.p, s->dYt.p, rows, s->loss.p, true);
     k_colsum<<<ew_grid(ctx, op), 256, 0, st>>>(rows, op, s->dY.p, s->gb3.p);
     // dW3 = dY^T H2 : [op, h]
     if ((r = gemm_tn(ctx, s->dYt.p, rows, s->H2t.p, rows, s->gW3.p, h, op, h, rows, s->err.p))) return r;
     // dH2 = dY W3 : [rows, h]  (B = W3^T stored [h][op])
-    if ((r = gemm_tn(ctx, s->dY.p, op, s->W3t.p, op, s->G.p, h, rows, h, op, s->err.p))) return r;
-    k_gelu_back<<<ew_grid(ctx, (long long)rows * h), 256, 0, st>>>(rows, valid, h, s->G.p, s->Z2.p, s->dZ.p, s->dZt.p,
+    if ((r = gemm_tn(ctx, s->dY.p, op, s->W3t.p, op, s->G.p, h, rows, h, op, s->err.p, &s->ws))) return r;
+    k_gelu_back<<<tile_grid(ctx, rows, h), kTileBlock, 0, st>>>(rows, valid, h, s->G.p, s->Z2.p, s->dZ.p, s->dZt.p,
                                                                     rows);
     k_colsum<<<ew_grid(ctx, h), 256, 0, st>>>(rows, h, s->dZ.p, s->gb2.p);
-    if ((r = gemm_tn(ctx, s->dZt.p, rows, s->H1t.p, rows, s->gW2.p, h, h, h, rows, s->err.p))) return r;
-    if ((r = gemm_tn(ctx, s->dZ.p, h, s->W2t.p, h, s->G.p, h, rows, h, h, s->err.p))) return r;
+    if ((r = gemm_tn(ctx, s->dZt.p, rows, s->H1t.p, rows, s->gW2.p, h, h, h, rows, s->err.p, &s->ws))) return r;
+    if ((r = gemm_tn(ctx, s->dZ.p, h, s->W2t.p, h, s->G.p, h, rows, h, h, s->err.p, &s->ws))) return r;
     // dZ1 reuses the dZ buffers
-    k_gelu_back<<<ew_grid(ctx, (long long)rows * h), 256, 0, st>>>(rows, valid, h, s->G.p, s->Z1.p, s->dZ.p, s->dZt.p,
+    k_gelu_back<<<tile_grid(ctx, rows, h), kTileBlock, 0, st>>>(rows, valid, h, s->G.p, s->Z1.p, s->dZ.p, s->dZt.p,
                                                                     rows);
     k_colsum<<<ew_grid(ctx, h), 256, 0, st>>>(rows, h, s->dZ.p, s->gb1.p);
-    if ((r = gemm_tn(ctx, s->dZt.p, rows, s->Xt.p, rows, s->gW1.p, in, h, in, rows, s->err.p))) return r;
+    if ((r = gemm_tn(ctx, s->dZt.p, rows, s->Xt.p, rows, s->gW1.p, in, h, in, rows, s->err.p, &s->ws))) return r;
     B2P_LAUNCH(ctx);
     ctx->launches += 6;
     return B2P_OK;
 }
 
+// One Adam step of all parameters; lr >= 0 sets the learning rate, a negative lr keeps the
+// one in device memory (the captured training epoch sets it before each replay).
 int adam_step(Ctx* ctx, MlpState* s, float lr) {
     s->step += 1;
-    const float b1t = 1.0f - powf(0.9f, (float)s->step), b2t = 1.0f - powf(0.999f, (float)s->step);
     const int in = s->in, h = s->hid, op = s->outp;
     cudaStream_t st = ctx->stream;
-    k_adam<<<ew_grid(ctx, (long long)h * in), 256, 0, st>>>((long long)h * in, in, s->W1.p, s->gW1.p, s->m1.p, s->v1.p, lr,
-                                                             b1t, b2t, s->W1h.p, s->W1t.p, h, h);
-    k_adam<<<ew_grid(ctx, (long long)h * h), 256, 0, st>>>((long long)h * h, h, s->W2.p, s->gW2.p, s->m2.p, s->v2.p, lr, b1t,
-                                                           b2t, s->W2h.p, s->W2t.p, h, h);
-    k_adam<<<ew_grid(ctx, (long long)op * h), 256, 0, st>>>((long long)op * h, h, s->W3.p, s->gW3.p, s->m3.p, s->v3.p, lr,
-                                                            b1t, b2t, s->W3h.p, s->W3t.p, op, s->out);
-    k_adam<<<ew_grid(ctx, h), 256, 0, st>>>(h, h, s->b1.p, s->gb1.p, s->mb1.p, s->vb1.p, lr, b1t, b2t, nullptr, nullptr, 0, 1);
-    k_adam<<<ew_grid(ctx, h), 256, 0, st>>>(h, h, s->b2.p, s->gb2.p, s->mb2.p, s->vb2.p, lr, b1t, b2t, nullptr, nullptr, 0, 1);
-    k_adam<<<ew_grid(ctx, op), 256, 0, st>>>(op, op, s->b3.p, s->gb3.p, s->mb3.p, s->vb3.p, lr, b1t, b2t, nullptr, nullptr, 0,
-                                             1);
+    const float* hy = s->hyper.p;
+    k_adam_begin<<<1, 1, 0, st>>>(s->dstep.p, s->hyper.p, lr);
+    k_adam<<<tile_grid(ctx, h, in), kTileBlock, 0, st>>>(h, in, s->W1.p, s->gW1.p, s->m1.p, s->v1.p, hy, s->W1h.p,
+                                                         s->W1t.p, h, h);
+    k_adam<<<tile_grid(ctx, h, h), kTileBlock, 0, st>>>(h, h, s->W2.p, s->gW2.p, s->m2.p, s->v2.p, hy, s->W2h.p,
+                                                        s->W2t.p, h, h);
+    k_adam<<<tile_grid(ctx, op, h), kTileBlock, 0, st>>>(op, h, s->W3.p, s->gW3.p, s->m3.p, s->v3.p, hy, s->W3h.p,
+                                                         s->W3t.p, op, s->out);
+    k_adam_vec<<<ew_grid(ctx, h), 256, 0, st>>>(h, s->b1.p, s->gb1.p, s->mb1.p, s->vb1.p, hy);
+    k_adam_vec<<<ew_grid(ctx, h), 256, 0, st>>>(h, s->b2.p, s->gb2.p, s->mb2.p, s->vb2.p, hy);
+    k_adam_vec<<<ew_grid(ctx, s->out), 256, 0, st>>>(s->out, s->b3.p, s->gb3.p, s->mb3.p, s->vb3.p, hy);
     B2P_LAUNCH(ctx);
-    ctx->launches += 6;
+    ctx->launches += 7;
     return B2P_OK;
 }
 
@@ -606,7 +692,7 @@ int stage_batch(Ctx* ctx, MlpState* s, const float* X, const float* T, int valid
     B2P_CUDA(ctx, cudaMemsetAsync(s->Xf.p, 0, sizeof(float) * (size_t)rows * in, st));
     B2P_CUDA(ctx, cudaMemcpyAsync(s->Xf.p, X, sizeof(float) * (size_t)valid * in, cudaMemcpyHostToDevice, st));
     if (T) B2P_CUDA(ctx, cudaMemcpyAsync(s->Tf.p, T, sizeof(float) * (size_t)valid * s->out, cudaMemcpyHostToDevice, st));
-    k_to_bf16<<<ew_grid(ctx, (long long)rows * in), 256, 0, st>>>(rows, in, s->Xf.p, in, s->Xh.p, in, s->Xt.p, rows);
+    k_to_bf16<<<tile_grid(ctx, rows, in), kTileBlock, 0, st>>>(rows, in, s->Xf.p, in, s->Xh.p, in, s->Xt.p, rows);
     B2P_LAUNCH(ctx);
     ctx->launches += 1;
     return B2P_OK;
@@ -616,12 +702,12 @@ int stage_batch(Ctx* ctx, MlpState* s, const float* X, const float* T, int valid
 int refresh_bf16(Ctx* ctx, MlpState* s) {
     const int in = s->in, h = s->hid, op = s->outp;
     cudaStream_t st = ctx->stream;
-    k_adam<<<ew_grid(ctx, (long long)h * in), 256, 0, st>>>((long long)h * in, in, s->W1.p, s->gW1.p, s->m1.p, s->v1.p, 0.f,
-                                                             1.f, 1.f, s->W1h.p, s->W1t.p, h, 0);
-    k_adam<<<ew_grid(ctx, (long long)h * h), 256, 0, st>>>((long long)h * h, h, s->W2.p, s->gW2.p, s->m2.p, s->v2.p, 0.f, 1.f,
-                                                           1.f, s->W2h.p, s->W2t.p, h, 0);
-    k_adam<<<ew_grid(ctx, (long long)op * h), 256, 0, st>>>((long long)op * h, h, s->W3.p, s->gW3.p, s->m3.p, s->v3.p, 0.f,
-                                                            1.f, 1.f, s->W3h.p, s->W3t.p, op, 0);
+    k_adam<<<tile_grid(ctx, h, in), kTileBlock, 0, st>>>(h, in, s->W1.p, s->gW1.p, s->m1.p, s->v1.p, nullptr, s->W1h.p,
+                                                         s->W1t.p, h, 0);
+    k_adam<<<tile_grid(ctx, h, h), kTileBlock, 0, st>>>(h, h, s->W2.p, s->gW2.p, s->m2.p, s->v2.p, nullptr, s->W2h.p,
+                                                        s->W2t.p, h, 0);
+    k_adam<<<tile_grid(ctx, op, h), kTileBlock, 0, st>>>(op, h, s->W3.p, s->gW3.p, s->m3.p, s->v3.p, nullptr, s->W3h.p,
+                                                         s->W3t.p, op, 0);
     B2P_LAUNCH(ctx);
     ctx->launches += 3;
     return B2P_OK;
@@ -726,11 +812,11 @@ int mlp_predict_warm(Ctx* ctx, const float* feat_host, int count, int n, int m, 
         B2P_CUDA(ctx, cudaMemsetAsync(s->Xf.p, 0, sizeof(float) * (size_t)rows * in, st));
         k_norm_rows<<<ew_grid(ctx, (long long)valid * in), 256, 0, st>>>(valid, in, raw.p + (size_t)off * in,
                                                                            s->in_mean.p, s->in_std.p, s->Xf.p);
-        k_to_bf16<<<ew_grid(ctx, (long long)rows * in), 256, 0, st>>>(rows, in, s->Xf.p, in, s->Xh.p, in, s->Xt.p, rows);
+        k_to_bf16<<<tile_grid(ctx, rows, in), kTileBlock, 0, st>>>(rows, in, s->Xf.p, in, s->Xh.p, in, s->Xt.p, rows);
         B2P_LAUNCH(ctx);
         ctx->launches += 2;
         if ((r = forward(ctx, s, rows, valid, false))) return r;
-        k_out_loss<<<ew_grid(ctx, (long long)rows * s->outp), 256, 0, st>>>(
+        k_out_loss<<<tile_grid(ctx, rows, s->outp), kTileBlock, 0, st>>>(
             rows, valid, s->out, s->outp, s->G.p, s->b3.p, nullptr, s->Y.p, nullptr, nullptr, 0, nullptr, false);
         k_denorm_warm<<<ew_grid(ctx, (long long)valid * s->out), 256, 0, st>>>(valid, s->outp, n, m, s->Y.p,
                                                                               s->out_mean.p, s->out_std.p, off, x0, y0,
@@ -773,12 +859,16 @@ int b2p_mlp_create(void* p, int in_dim, int hidden, int out_dim, uint64_t seed) 
     for (auto* d : {&s->W3h, &s->W3t}) B2P_CUDA(ctx, d->reserve(op * h));
     B2P_CUDA(ctx, s->loss.reserve(1));
     B2P_CUDA(ctx, s->err.reserve(1));
+    B2P_CUDA(ctx, s->hyper.reserve(4));
+    B2P_CUDA(ctx, s->dstep.reserve(1));
     cudaStream_t st = ctx->stream;
     for (auto* d : {&s->m1, &s->v1, &s->gW1}) B2P_CUDA(ctx, cudaMemsetAsync(d->p, 0, d->bytes(), st));
     for (auto* d : {&s->m2, &s->v2, &s->gW2, &s->m3, &s->v3, &s->gW3}) B2P_CUDA(ctx, cudaMemsetAsync(d->p, 0, d->bytes(), st));
     for (auto* d : {&s->mb1, &s->vb1, &s->gb1, &s->mb2, &s->vb2, &s->gb2, &s->mb3, &s->vb3, &s->gb3})
         B2P_CUDA(ctx, cudaMemsetAsync(d->p, 0, d->bytes(), st));
     B2P_CUDA(ctx, cudaMemsetAsync(s->err.p, 0, sizeof(int), st));
+    B2P_CUDA(ctx, cudaMemsetAsync(s->dstep.p, 0, sizeof(long long), st));
+    B2P_CUDA(ctx, cudaMemsetAsync(s->hyper.p, 0, 4 * sizeof(float), st));
     k_init_uniform<<<ew_grid(ctx, h * in), 256, 0, st>>>(h * in, 1.0f / std::sqrt((float)in), seed * 6 + 1, s->W1.p, h * in);
     k_init_uniform<<<ew_grid(ctx, h), 256, 0, st>>>(h, 1.0f / std::sqrt((float)in), seed * 6 + 2, s->b1.p, h);
     k_init_uniform<<<ew_grid(ctx, h * h), 256, 0, st>>>(h * h, 1.0f / std::sqrt((float)h), seed * 6 + 3, s->W2.p, h * h);
@@ -840,7 +930,7 @@ int b2p_mlp_infer(void* p, const float* X, int N, float* Y_out) {
         const int rows = (valid + 7) & ~7;
         if ((r = stage_batch(ctx, s, X + (size_t)off * s->in, nullptr, valid, rows))) return r;
         if ((r = forward(ctx, s, rows, valid, false))) return r;
-        k_out_loss<<<ew_grid(ctx, (long long)rows * s->outp), 256, 0, ctx->stream>>>(
+        k_out_loss<<<tile_grid(ctx, rows, s->outp), kTileBlock, 0, ctx->stream>>>(
             rows, valid, s->out, s->outp, s->G.p, s->b3.p, nullptr, s->Y.p, nullptr, nullptr, 0, nullptr, false);
         B2P_LAUNCH(ctx);
         ctx->launches += 1;
@@ -926,13 +1016,11 @@ int b2p_mlp_train(void* p, int epochs, int batch, float lr_start, float lr_end, 
     std::vector<int32_t> order(N);
     std::iota(order.begin(), order.end(), 0);
     std::mt19937_64 rng(seed);
-    double loss = 0.0;
-    for (int ep = 0; ep < epochs; ++ep) {
-        std::shuffle(order.begin(), order.end(), rng);
-        B2P_CUDA(ctx, cudaMemcpyAsync(s->perm.p, order.data(), sizeof(int32_t) * N, cudaMemcpyHostToDevice, st));
-        const double cosw = 0.5 * (1.0 + std::cos(3.14159265358979323846 * ep / epochs));
-        const float lr = (float)(lr_end + (lr_start - lr_end) * cosw);
-        B2P_CUDA(ctx, cudaMemsetAsync(s->loss.p, 0, sizeof(double), st));
+    // One epoch is a fixed sequence of launches -- the sample order lives in perm and the
+    // learning rate in device memory -- so it is captured once as a CUDA graph and replayed
+    // every epoch: no per-step host work (launches, tensor-map encoding) on the critical path.
+    auto epoch_body = [&]() -> int {
+        int q;
         for (int off = 0; off < N; off += batch) {
             const int valid = std::min(batch, N - off);
             const int rows = (valid + 7) & ~7;
@@ -940,18 +1028,69 @@ int b2p_mlp_train(void* p, int epochs, int batch, float lr_start, float lr_end, 
                                                                               s->Xf.p);
             k_gather_rows<<<ew_grid(ctx, (long long)rows * out), 256, 0, st>>>(valid, rows, out, s->perm.p + off,
                                                                                s->DT.p, s->Tf.p);
-            k_to_bf16<<<ew_grid(ctx, (long long)rows * in), 256, 0, st>>>(rows, in, s->Xf.p, in, s->Xh.p, in, s->Xt.p,
-                                                                           rows);
+            k_to_bf16<<<tile_grid(ctx, rows, in), kTileBlock, 0, st>>>(rows, in, s->Xf.p, in, s->Xh.p, in, s->Xt.p,
+                                                                        rows);
             B2P_LAUNCH(ctx);
             ctx->launches += 3;
-            if ((r = forward(ctx, s, rows, valid, true))) return r;
-            if ((r = backward(ctx, s, rows, valid))) return r;
-            if ((r = adam_step(ctx, s, lr))) return r;
+            if ((q = forward(ctx, s, rows, valid, true))) return q;
+            if ((q = backward(ctx, s, rows, valid))) return q;
+            if ((q = adam_step(ctx, s, -1.0f))) return q;
         }
+        return B2P_OK;
+    };
+    const int steps_per_epoch = (N + batch - 1) / batch;
+    if (!s->epoch_exec || s->epoch_n != N || s->epoch_batch != batch) {
+        if (s->epoch_exec) {
+            cudaGraphExecDestroy(s->epoch_exec);
+            s->epoch_exec = nullptr;
+        }
+        // outside the capture: kernel attributes and the split-K workspace of every GEMM shape
+        // (one forward / backward of a full batch; no parameter changes)
+        const int rows0 = (std::min(batch, N) + 7) & ~7;
+        if ((r = forward(ctx, s, rows0, std::min(batch, N), true))) return r;
+        if ((r = backward(ctx, s, rows0, std::min(batch, N)))) return r;
+        B2P_CUDA(ctx, cudaStreamSynchronize(st));
+        const long long launches0 = ctx->launches, step0 = s->step;
+        cudaGraph_t graph = nullptr;
+        B2P_CUDA(ctx, cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+        const int body = epoch_body();
+        cudaError_t ce = cudaStreamEndCapture(st, &graph);
+        if (body != B2P_OK) {
+            if (graph) cudaGraphDestroy(graph);
+            return body;
+        }
+        if (ce != cudaSuccess) {
+            ctx->err = std::string("b2p_mlp_train: epoch capture: ") + cudaGetErrorString(ce);
+            return B2P_EXECUTION_FAILED;
+        }
+        ce = cudaGraphInstantiate(&s->epoch_exec, graph, 0);
+        cudaGraphDestroy(graph);
+        if (ce != cudaSuccess) {
+            s->epoch_exec = nullptr;
+            ctx->err = std::string("b2p_mlp_train: epoch graph: ") + cudaGetErrorString(ce);
+            return B2P_EXECUTION_FAILED;
+        }
+        s->epoch_launches = ctx->launches - launches0;
+        ctx->launches = launches0;  // counted per replay below
+        s->step = step0;
+        s->epoch_n = N;
+        s->epoch_batch = batch;
+    }
+    double loss = 0.0;
+    for (int ep = 0; ep < epochs; ++ep) {
+        std::shuffle(order.begin(), order.end(), rng);
+        B2P_CUDA(ctx, cudaMemcpyAsync(s->perm.p, order.data(), sizeof(int32_t) * N, cudaMemcpyHostToDevice, st));
+        const double cosw = 0.5 * (1.0 + std::cos(3.14159265358979323846 * ep / epochs));
+        const float lr = (float)(lr_end + (lr_start - lr_end) * cosw);
+        B2P_CUDA(ctx, cudaMemcpyAsync(s->hyper.p, &lr, sizeof(float), cudaMemcpyHostToDevice, st));
+        B2P_CUDA(ctx, cudaMemsetAsync(s->loss.p, 0, sizeof(double), st));
+        B2P_CUDA(ctx, cudaGraphLaunch(s->epoch_exec, st));
+        ctx->launches += s->epoch_launches;
+        s->step += steps_per_epoch;
         if (ep == epochs - 1) {
             B2P_CUDA(ctx, cudaMemcpyAsync(&loss, s->loss.p, sizeof(double), cudaMemcpyDeviceToHost, st));
         }
-        if ((r = check_err(ctx, s))) return r;  // also bounds the queue of launches to one epoch
+        if ((r = check_err(ctx, s))) return r;  // one sync per epoch: the order and lr buffers are reused
     }
     if (loss_out) *loss_out = (float)(loss / ((double)N * out));
     return B2P_OK;
