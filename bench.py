@@ -41,7 +41,7 @@ sys.path.insert(0, str(ROOT))
 # extrapolates the reference CPU solver's per-iteration cost over this many
 # iterations -- generous to the CPU: the reference's own vanilla PDHG needs far
 # more iterations and never reaches 1e-6 on these LPs.
-HALPERN_ITERS = {"block_angular": 6784, "random_sparse": 5056, "refinery_learned": 65388,
+HALPERN_ITERS = {"block_angular": 6784, "random_sparse": 5056, "refinery_learned": 65388, "uneven_batch": 6207,
                  # mixed engine to 1e-8 (the FP64 leg of this workload was not run)
                  "ill_conditioned": 1230784}
 
@@ -327,6 +327,55 @@ def cpu_reference_sample(lp, sample_iters, iters_needed):
             "per_iteration_ms": per_iter * 1e3, "setup_s": setup}
 
 
+def _batch_ref_worker(task):
+    """One bounded reference CPUFirstOrderSolver sample on instance i of a batched workload."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    from oracle_lib import RefLib  # oracle: reference arm only
+    workload, count, i, sample = task
+    args = argparse.Namespace(workload=workload, batch_count=count)
+    _, lps, _, _, _ = batch_lps(args)
+    ref = RefLib()
+    r1 = ref.fo_solve(lps[i], max_iterations=1)
+    r2 = ref.fo_solve(lps[i], max_iterations=1 + sample)
+    ran = max(1, int(r2.get("iterations", 1 + sample)) - 1)
+    return r1["solve_time_ms"] / 1e3, (r2["solve_time_ms"] - r1["solve_time_ms"]) / ran / 1e3
+
+
+def run_reference_batch(args):
+    """Reference arm of the batched workloads: the reference's CPU PDHG on the workload's
+    instances, one per host core in parallel; per-LP time = setup + per-iteration cost x the
+    iterations the FP64 engine needs (an extrapolation: the reference's own vanilla PDHG has
+    no relative-KKT stop and does not reach the tolerance on these LPs)."""
+    import multiprocessing as mp
+    _, lps, stds, _, cfg = batch_lps(args)
+    cores = os.cpu_count() or 1
+    iters = HALPERN_ITERS.get(args.workload, 6207)
+    sample = 4000
+    vals = []
+    t0 = time.perf_counter()
+    stride = max(1, len(lps) // (cores * max(1, args.steps)))
+    with mp.get_context("spawn").Pool(cores) as pool:
+        pool.map(_batch_ref_worker, [(args.workload, args.batch_count, 0, 10)] * cores)  # warm-up
+        for step in range(args.steps):
+            idx = [((step * cores + c) * stride) % len(lps) for c in range(cores)]
+            out = pool.map(_batch_ref_worker, [(args.workload, args.batch_count, i, sample) for i in idx])
+            per_lp = [a + b * iters for a, b in out]
+            vals.append(len(out) / max(per_lp))
+    wall = time.perf_counter() - t0
+    v = statistics.median(vals)
+    cb = {"value": v, "unit": "LPs/s", "cores": cores, "kind": "reference",
+          "sample": (f"reference CPUFirstOrderSolver, {cores} processes x 1 instance each: runs of 1 and {1 + sample} "
+                     f"iterations; per-LP time = setup + {iters} x per-iteration; {wall:.1f} s wall"),
+          "extrapolation": {"iterations": iters, "source": "mean iterations of this engine's plain FP64 solve of the "
+                            "workload (a different algorithm: restarted Halpern PDHG with scaling)"}}
+    line = {"metric": metric_for(args), "value": v, "unit": "LPs/s", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 / v, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator, no dataset)", "config": cfg,
+            "impl": "reference", "cpu_baseline": cb,
+            "e2e": {"value": v, "unit": "LPs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", 0))
     if rank != 0:
@@ -353,18 +402,18 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
-def batch_lps(args):
+def batch_lps(args, seed_offset=0):
     """(standard-form instances, shared matrix or None, config) of a batched workload."""
     import __graft_entry__ as g
     b2p = g.load_package()
     if args.workload == "uneven_batch":
-        lps = b2p.lpgen.uneven_batch(args.batch_count, seed=2)
+        lps = b2p.lpgen.uneven_batch(args.batch_count, seed=2 + seed_offset)
         stds = [lp.standard() for lp in lps]
         cfg = {"workload": "uneven_batch", "count": len(stds), "m": "logU(50,2000)", "n": "m*U(2,5)",
                "nnz_per_col": "4-10", "seed": 2, "nnz_total": int(sum(s.nnz for s in stds))}
         return b2p, lps, stds, None, cfg
     fam = b2p.lpgen.RefineryFamily()
-    p = fam.sample_params(args.batch_count, seed=20001)
+    p = fam.sample_params(args.batch_count, seed=20001 + seed_offset)
     lps = [fam.instance(q) for q in p]
     stds = [lp.standard() for lp in lps]
     cfg = {"workload": "refinery_family_cold", "count": len(stds), "m": fam.m, "n": fam.n,
@@ -385,53 +434,112 @@ def upload_batch(ctx, stds, shared):
 
 
 def run_batch_workload(args):
+    """configs[2] (uneven_batch: 4096 LPs of uneven size, each its own matrix) or the
+    random-structure refinery family (one shared matrix), cold start: mixed precision
+    timed for --steps, plain FP64 for --compare-steps, end to end for --e2e-steps; one
+    replica per GPU on its own seed (weak scaling)."""
     import torch
-    torch.cuda.set_device(0)
+    rank, world, local = dist_setup(args.gpus)
+    torch.cuda.set_device(local)
     torch.cuda.set_stream(torch.cuda.Stream())
-    b2p, lps, stds, shared, cfg = batch_lps(args)
-    ctx = b2p.Context(0)
+    b2p, lps, stds, shared, cfg = batch_lps(args, seed_offset=1000 * rank)
+    ctx = b2p.Context(local)
     ctx.set_stream(torch.cuda.current_stream().cuda_stream)
     upload_batch(ctx, stds, shared)
-    common = dict(eps=args.eps, max_iterations=400000)
-    stream = torch.cuda.current_stream()
-    res = {}
-    for prec in ("fp32", "fp64"):
-        # warm-up of this precision (autotuning and allocations happen here, not in the timed steps)
-        for _ in range(args.warmup):
-            ctx.batch_solve(precision=prec, **common)
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        torch.cuda.synchronize()
-        e0.record(stream)
-        for _ in range(args.steps):
-            summ, per, x, y = ctx.batch_solve(precision=prec, **common)
-        e1.record(stream)
-        torch.cuda.synchronize()
-        ms = e0.elapsed_time(e1) / args.steps
-        res[prec] = {"value": len(stds) / (ms / 1e3), "ms_per_step": ms, "solved": int((per["status"] == 0).sum()),
+    judge = dict(eps=args.eps, eps_objective=args.eps_objective)
+    cap = 400000
+    for _ in range(args.warmup):
+        for prec in ("fp32", "fp64"):
+            ctx.batch_solve(precision=prec, max_iterations=2048, outputs=False, **judge)
+    uuid = None
+    try:
+        uuid = "GPU-" + str(torch.cuda.get_device_properties(local).uuid)
+    except Exception:
+        pass
+    res, clocks = {}, None
+    for prec, k in (("fp32", args.steps), ("fp64", args.compare_steps)):
+        if k <= 0:
+            continue
+        sampler = ClockSampler(uuid) if prec == "fp32" else None
+        if sampler:
+            sampler.start()
+        ms, (summ, per, _, _) = timed_leg(ctx, torch, world, k,
+                                          lambda: ctx.batch_solve(precision=prec, max_iterations=cap, outputs=False,
+                                                                  **judge))
+        if sampler:
+            clocks = sampler.stop()
+        solved = sum_over_ranks(float((per["status"] == 0).sum()), world)
+        res[prec] = {"value": solved * k / (ms / 1e3), "unit": "LPs/s", "steps": k, "ms_per_step": ms / k,
+                     "solved": int(solved), "instances": len(stds) * world,
                      "iterations_mean": float(per["iterations"].mean()), "iterations_max": int(per["iterations"].max()),
-                     "worst_rel_kkt": float(per["rel_kkt"].max()), "kernel_launches": summ["kernel_launches"],
-                     "tuned_threads_chunk": summ["step_size"]}
-    # algorithmic bytes of the mixed run: every instance iteration streams its matrix (both
-    # orientations, FP32 value + int32 index) and its vectors once
-    summ, per, x, y = ctx.batch_solve(precision="fp32", **common)
-    nn = np.array([s.nnz for s in stds], float)
-    mm = np.array([s.m for s in stds], float)
-    nv = np.array([s.n for s in stds], float)
-    per_iter = nn * 16 + 4 * (mm + nv) + nv * 56 + mm * 41
-    alg = float((per["iterations"] * per_iter).sum())
+                     "worst_rel_kkt": float(per["rel_kkt"].max()), "kernel_ms": summ["kernel_time_ms"],
+                     "kernel_launches": summ["kernel_launches"], "tuned_threads_chunk": summ["step_size"],
+                     "trace": trace_summary(*ctx.batch_trace(), len(stds))}
+        if prec == "fp32":
+            it_total = float(per["iterations"].sum())
+            per_inst_iters = per["iterations"].astype(float)
+            kern_ms = summ["kernel_time_ms"]
+            launches = int(summ["kernel_launches"]) * k
+    # end to end: pinned host instance data -> batch upload -> mixed solve -> x, y to host
+    pin = {k: torch.from_numpy(np.ascontiguousarray(np.concatenate([getattr(s_, k) for s_ in stds]))).pin_memory()
+           for k in ("b", "c", "lb", "ub", "is_eq")}
+    h2d = sum(t.numel() * t.element_size() for t in pin.values())
+    mats = ([(shared.m, shared.n, shared.rowptr, shared.colidx, shared.vals)] if shared is not None
+            else [(s_.m, s_.n, s_.rowptr, s_.colidx, s_.vals) for s_ in stds])
+    h2d += sum(q[2].nbytes + q[3].nbytes + q[4].nbytes for q in mats)
+    inst = np.zeros(len(stds), np.int32) if shared is not None else np.arange(len(stds), dtype=np.int32)
+    d2h = 8 * sum(s_.n + s_.m for s_ in stds)
+
+    def e2e_step():
+        ctx.batch_upload(mats, inst, pin["b"].numpy(), pin["c"].numpy(), pin["lb"].numpy(), pin["ub"].numpy(),
+                         pin["is_eq"].numpy())
+        return ctx.batch_solve(precision="fp32", max_iterations=cap, **judge)
+
+    e2e = {"value": None, "skipped": "--e2e-steps 0", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h}
+    if args.e2e_steps > 0:
+        e2e_ms, (_, eper, _, _) = timed_leg(ctx, torch, world, args.e2e_steps, e2e_step)
+        esolved = sum_over_ranks(float((eper["status"] == 0).sum()), world)
+        e2e = {"value": esolved * args.e2e_steps / (e2e_ms / 1e3), "unit": "LPs/s", "h2d_bytes_per_step": h2d,
+               "d2h_bytes_per_step": d2h, "steps": args.e2e_steps, "ms_per_step": e2e_ms / args.e2e_steps,
+               "solved": int(esolved)}
+    # roofline of k_batch_chunk<float>: algorithmic bytes of every instance-iteration (12 B per
+    # nonzero, 24 B per column, 16 B per row) over its kernel time; the bound is HBM when the
+    # matrices and vectors the resident instances stream exceed L2, else L2
+    per_iter = np.array([12.0 * s_.nnz + 24.0 * s_.n + 16.0 * s_.m for s_ in stds])
+    alg = float((per_inst_iters * per_iter).sum())
     peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
     peak = peaks.get("hbm_gbs", 6650.0)
-    achieved = alg / (res["fp32"]["ms_per_step"] / 1e3) / 1e9
-    line = {"metric": metric_for(args), "value": res["fp32"]["value"], "unit": "LPs/s", "n_gpus": 1, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": res["fp32"]["ms_per_step"], "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32 values + f64 iterates/KKT",
-            "data": "synthetic (seeded generator, no dataset)", "config": cfg, "mixed": res["fp32"], "fp64": res["fp64"],
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                         "note": "algorithmic bytes of every instance-iteration over the whole batched solve; "
-                                 "the shared-memory gathers and an L2-resident working set make this an upper "
-                                 "bound on DRAM traffic"}}
-    print(json.dumps(line), flush=True)
+    achieved = alg / (kern_ms / 1e3) / 1e9
+    resident = 2 * 148  # two CTAs per SM, one instance each
+    vec = np.array([24.0 * s_.n + 16.0 * s_.m for s_ in stds])
+    mat = np.array([12.0 * s_.nnz for s_ in stds])
+    top = np.argsort(-(vec + mat))[:resident]
+    hot = float(vec[top].sum() + (mat[0] if shared is not None else mat[top].sum()))
+    bound = "hbm" if hot > 126e6 else "l2"
+    roofline = {"bound": bound, "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": None, "kernel": "k_batch_chunk<float>",
+                "algorithmic_bytes_per_instance_iteration_mean": float(per_iter.mean()),
+                "resident_working_set_bytes": hot,
+                "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if peaks else "fallback 6650 (of fallback)"}
+    cpu = None
+    if rank == 0 and world == 1 and "fp64" in res:
+        cpu = cpu_reference_sample(lps[0], 2000, int(res["fp64"]["iterations_mean"]))
+    if rank == 0:
+        line = {"metric": metric_for(args), "value": res["fp32"]["value"], "unit": "LPs/s", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": res["fp32"]["ms_per_step"],
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f32 (SpMV, vectors) + f64 (scaling, KKT, re-centring)",
+                "data": "synthetic (seeded generator, no dataset)",
+                "config": dict(cfg, parallelism=f"replicas x{world}", eps_rel_kkt=args.eps,
+                               eps_objective=args.eps_objective,
+                               steps={"mixed (value)": args.steps, "fp64": args.compare_steps, "e2e": args.e2e_steps}),
+                "mixed": res["fp32"], "fp64": res.get("fp64"), "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu,
+                "gpu_launches": launches, "clocks": clocks}
+        print(json.dumps(line), flush=True)
     ctx.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
 
 
 def learned_setup(args, rank):
@@ -724,6 +832,8 @@ def main():
             return
         if args.workload == "refinery_learned":
             run_reference_learned(args)
+        elif args.workload in ("uneven_batch", "refinery"):
+            run_reference_batch(args)
         else:
             run_reference(args)
         return

@@ -213,3 +213,20 @@ def test_batch_autotuned_shape(ctx, lpgen, tmp_path, monkeypatch):
     summ2, per2, _, _ = ctx.batch_solve(precision="fp32", eps=1e-6, max_iterations=100000, outputs=False)
     assert summ2["step_size"] == summ["step_size"]
     assert np.array_equal(per2["iterations"], per["iterations"])  # deterministic
+
+
+def test_batch_trace_and_objectives(ctx, lpgen):
+    """The active-instance trace of a solve runs from the batch size down to zero in
+    increasing time, and the per-instance objectives agree with the oracle's."""
+    lps = lpgen.uneven_batch(24, m_hi=400, seed=45)
+    stds = upload_lps(ctx, lps)
+    _, per, x, y = ctx.batch_solve(precision="fp64", eps=1e-7, max_iterations=200000)
+    t, active = ctx.batch_trace()
+    assert active[0] == len(stds) and active[-1] == 0
+    assert np.all(np.diff(active) <= 0) and np.all(np.diff(t) >= 0)
+    obj = ctx.batch_objectives()
+    for i, (s, (xi, yi)) in enumerate(zip(stds, split(stds, x, y))):
+        k = pdlp_oracle.kkt(s, xi, yi)
+        assert abs(obj["pobj"][i] - k["pobj"]) <= 1e-9 * max(1.0, abs(k["pobj"]))
+        assert abs(obj["dobj"][i] - k["dobj"]) <= 1e-6 * max(1.0, abs(k["dobj"]))
+        assert 0.0 <= obj["obj_err"][i] < 1e-3
