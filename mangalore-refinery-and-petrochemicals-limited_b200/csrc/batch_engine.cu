@@ -51,6 +51,7 @@
 #include <cub/cub.cuh>
 
 #include <algorithm>
+#include <type_traits>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
@@ -113,6 +114,8 @@ struct BatchWork {
     bool solved = false;
     int tuned_threads[2] = {0, 0};  // block size per precision (0 = not tuned yet)
     int tuned_chunk[2] = {2048, 2048};  // iterations per chunk launch per precision
+    int tuned_w[2] = {1, 1};        // SELL entry order per precision
+    int ell_w = 1;                  // entry order the SELL copies hold now
     DBuf<int32_t> list;             // instances re-initialised by a subset solve
     // active-instance trace of the last solve: host time (ms from the first graph launch of
     // the solve) and instances still active after each graph launch (a fallback run continues
@@ -201,30 +204,55 @@ __device__ __forceinline__ void block_sums(double (&v)[NV], double* sh /* [32*NV
     }
 }
 
-// One lane's row of a SELL-32 slice: v / ix point at the lane's first entry, the
-// next entry of the same row is 32 elements further.  Sequential sum in entry order.
+// One lane's row of a SELL-32 slice (len entries per lane, even).  W = 1: v / ix point at
+// the lane's first entry and entry q sits 32 q further.  W = 2: entries are stored in
+// pairs -- pair t of lane l at slice + 64 t + 2 l -- so one 8- (FP32) or 16-byte (FP64)
+// value load and one 4-byte index load fetch two entries; v / ix point at the lane's
+// first pair.  Sequential sum in entry order in both layouts (bit-identical results).
 // Entries are taken in batches of B (8 in FP32, 4 in FP64, the most the register
 // budget of two 512-thread CTAs per SM holds without spilling in the loop): every
 // value and index load of a batch (the last batch predicated on the row's length)
 // is issued before the first gather that needs one, so a slice of up to B entries
 // per lane costs one L2 round trip and a longer one a round trip per batch.
-template <typename MT>
+template <typename MT, int W>
 __device__ __forceinline__ MT ell_dot(const MT* __restrict__ v, const uint16_t* __restrict__ ix, int len,
                                       const MT* __restrict__ g) {
     constexpr int B = sizeof(MT) == 4 ? 8 : 4;
     MT s = (MT)0;
-    for (int q = 0; q < len; q += B) {
-        MT vv[B];
-        unsigned ii[B];
+    if constexpr (W == 1) {
+        for (int q = 0; q < len; q += B) {
+            MT vv[B];
+            unsigned ii[B];
 #pragma unroll
-        for (int u = 0; u < B; ++u) {
-            const bool h = q + u < len;
-            vv[u] = h ? v[(q + u) * 32] : (MT)0;
-            ii[u] = h ? (unsigned)ix[(q + u) * 32] : 0u;
+            for (int u = 0; u < B; ++u) {
+                const bool h = q + u < len;
+                vv[u] = h ? v[(q + u) * 32] : (MT)0;
+                ii[u] = h ? (unsigned)ix[(q + u) * 32] : 0u;
+            }
+#pragma unroll
+            for (int u = 0; u < B; ++u)
+                if (q + u < len) s += vv[u] * g[ii[u]];
         }
+    } else {
+        typedef typename std::conditional<sizeof(MT) == 4, float2, double2>::type MT2;
+        constexpr int P = B / 2;  // pairs per batch
+        const int np = len >> 1;
+        for (int t = 0; t < np; t += P) {
+            MT2 vv[P];
+            unsigned ii[P];
 #pragma unroll
-        for (int u = 0; u < B; ++u)
-            if (q + u < len) s += vv[u] * g[ii[u]];
+            for (int u = 0; u < P; ++u) {
+                const bool h = t + u < np;
+                vv[u] = h ? *reinterpret_cast<const MT2*>(v + (t + u) * 64) : MT2{(MT)0, (MT)0};
+                ii[u] = h ? *reinterpret_cast<const unsigned*>(ix + (t + u) * 64) : 0u;
+            }
+#pragma unroll
+            for (int u = 0; u < P; ++u)
+                if (t + u < np) {
+                    s += vv[u].x * g[ii[u] & 0xFFFFu];
+                    s += vv[u].y * g[ii[u] >> 16];
+                }
+        }
     }
     return s;
 }
@@ -467,7 +495,7 @@ __device__ __noinline__ void check_instance(const BArgs& a, int inst, int m, int
 // size, up to 512 threads, two CTAs per SM) while many instances are active and as
 // k_batch_chunk_wide (1024 threads, one CTA per SM) once no more than one instance
 // per SM is left, so the last, slowest instances iterate with twice the threads.
-template <typename MT>
+template <typename MT, int W>
 __device__ __forceinline__ void batch_chunk_body(const BArgs& a, int chunk) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ double red[32 * 7];
@@ -532,7 +560,7 @@ __device__ __forceinline__ void batch_chunk_body(const BArgs& a, int chunk) {
                 const int64_t p0 = csp[sl];
                 const int len = (int)((csp[sl + 1] - p0) >> 5);
                 const MT s = len <= kLongSlice
-                                 ? ell_dot<MT>(cev + p0 + lane, a.c_eidx + p0 + lane, len, ys)
+                                 ? ell_dot<MT, W>(cev + p0 + W * lane, a.c_eidx + p0 + W * lane, len, ys)
                                  : long_slice_dot<MT>(stv, a.t_rowptr, a.t_colidx, co + (sl << 5), min(32, n - (sl << 5)),
                                                       ro, ys, lane);
                 if (valid) {
@@ -561,7 +589,7 @@ __device__ __forceinline__ void batch_chunk_body(const BArgs& a, int chunk) {
                 const int64_t p0 = rsp[sl];
                 const int len = (int)((rsp[sl + 1] - p0) >> 5);
                 const MT s = len <= kLongSlice
-                                 ? ell_dot<MT>(rev + p0 + lane, a.r_eidx + p0 + lane, len, xhs)
+                                 ? ell_dot<MT, W>(rev + p0 + W * lane, a.r_eidx + p0 + W * lane, len, xhs)
                                  : long_slice_dot<MT>(sv, a.rowptr, a.colidx, ro + (sl << 5), min(32, m - (sl << 5)),
                                                       co, xhs, lane);
                 if (valid) {
@@ -660,14 +688,14 @@ __device__ __forceinline__ void batch_chunk_body(const BArgs& a, int chunk) {
     }
 }
 
-template <typename MT>
+template <typename MT, int W>
 __global__ void __launch_bounds__(512, 2) k_batch_chunk(const __grid_constant__ BArgs a, int chunk) {
-    batch_chunk_body<MT>(a, chunk);
+    batch_chunk_body<MT, W>(a, chunk);
 }
 
-template <typename MT>
+template <typename MT, int W>
 __global__ void __launch_bounds__(1024, 1) k_batch_chunk_wide(const __grid_constant__ BArgs a, int chunk) {
-    batch_chunk_body<MT>(a, chunk);
+    batch_chunk_body<MT, W>(a, chunk);
 }
 
 // Order-preserving compaction of the active list (one CTA).
@@ -830,9 +858,10 @@ __global__ void k_batch_power(int nmat, const int32_t* __restrict__ mat_m, const
 
 // SELL-32 copy of one orientation, CTA per matrix: every lane slot of every slice
 // (rows past the matrix end and entries past a row's end are zero padding with
-// local index 0).  ptr / idx / v64 / v32 are the CSR of that orientation in
-// global numbering; `other_off` localises its indices.
-__global__ void k_fill_ell(int nmat, const int32_t* __restrict__ dim, const int64_t* __restrict__ off,
+// local index 0), in the W = 1 or W = 2 (pairs) order of ell_dot.  ptr / idx / v64 /
+// v32 are the CSR of that orientation in global numbering; `other_off` localises its
+// indices.
+__global__ void k_fill_ell(int W, int nmat, const int32_t* __restrict__ dim, const int64_t* __restrict__ off,
                            const int64_t* __restrict__ other_off, const int64_t* __restrict__ s_off,
                            const int64_t* __restrict__ sptr, const int32_t* __restrict__ ptr,
                            const int32_t* __restrict__ idx, const double* __restrict__ v64,
@@ -853,7 +882,7 @@ __global__ void k_fill_ell(int nmat, const int32_t* __restrict__ dim, const int6
                 e1 = ptr[base + li + 1];
             }
             for (int q = 0; q < len; ++q) {
-                const int64_t pos = p0 + 32 * (int64_t)q + lane;
+                const int64_t pos = W == 1 ? p0 + 32 * (int64_t)q + lane : p0 + 64 * (int64_t)(q >> 1) + 2 * lane + (q & 1);
                 if (e + q < e1) {
                     eidx[pos] = (uint16_t)(idx[e + q] - ob);
                     ev64[pos] = v64[e + q];
@@ -1001,7 +1030,7 @@ __global__ void k_batch_unscale(BArgs a, int count, const double* __restrict__ x
 
 // ------------------------------------------------------------------ host side
 struct TuneCfg {
-    int threads, chunk;
+    int threads, chunk, w;  // CTA size, iterations per chunk launch, SELL entries per lane load (1 or 2)
 };
 
 std::string cache_path() {
@@ -1016,7 +1045,7 @@ std::string batch_key(BatchWork* w, int precision) {
     double mean_m = (double)w->inst_m / w->count, mean_n = (double)w->inst_n / w->count;
     double nnz_col = (double)w->nnz / std::max<int64_t>(w->tot_n, 1);
     std::ostringstream os;
-    os << "batch4_p" << precision << "_c" << (int)std::log2(std::max(1, w->count)) << "_m"
+    os << "batch5_p" << precision << "_c" << (int)std::log2(std::max(1, w->count)) << "_m"
        << (int)std::log2(mean_m + 1) << "_n" << (int)std::log2(mean_n + 1) << "_k" << (int)std::lround(nnz_col) << "_M"
        << w->max_m << "_N" << w->max_n << "_shared" << (w->nmat == 1 && w->count > 1);
     return os.str();
@@ -1030,7 +1059,7 @@ bool cache_lookup(const std::string& key, TuneCfg* out) {
         std::string k;
         TuneCfg c;
         if (!(is >> k) || k != key) continue;
-        if (is >> c.threads >> c.chunk) {
+        if (is >> c.threads >> c.chunk >> c.w) {
             *out = c;
             return true;
         }
@@ -1046,7 +1075,7 @@ void cache_store(const std::string& key, const TuneCfg& c) {
         if (std::system(cmd.c_str()) != 0) return;
     }
     std::ofstream f(p, std::ios::app);
-    f << key << " " << c.threads << " " << c.chunk << "\n";
+    f << key << " " << c.threads << " " << c.chunk << " " << c.w << "\n";
 }
 
 template <typename MT>
@@ -1136,14 +1165,33 @@ int init_instances(Ctx* ctx, BatchWork* w, const b2p_params* p, const double* x0
     return B2P_OK;
 }
 
+// Rewrites both SELL copies in entry order W (1 or 2); the slice pointers (even lengths)
+// serve both orders.
+int refill_ell(Ctx* ctx, BatchWork* w, int W) {
+    if (w->ell_w == W) return B2P_OK;
+    cudaStream_t s = ctx->stream;
+    const unsigned gmat = (unsigned)std::min(w->nmat, ctx->sm_count * 8);
+    k_fill_ell<<<gmat, 256, 0, s>>>(W, w->nmat, w->mat_m.p, w->mat_row_off.p, w->mat_col_off.p, w->mat_rs_off.p,
+                                     w->r_sptr.p, w->rowptr.p, w->colidx.p, w->sv64.p, w->sv32.p, w->r_eidx.p,
+                                     w->r_ev64.p, w->r_ev32.p);
+    k_fill_ell<<<gmat, 256, 0, s>>>(W, w->nmat, w->mat_n.p, w->mat_col_off.p, w->mat_row_off.p, w->mat_cs_off.p,
+                                     w->c_sptr.p, w->t_rowptr.p, w->t_colidx.p, w->stv64.p, w->stv32.p, w->c_eidx.p,
+                                     w->c_ev64.p, w->c_ev32.p);
+    B2P_LAUNCH(ctx);
+    ctx->launches += 2;
+    w->ell_w = W;
+    return B2P_OK;
+}
+
 // Times each block size on a size-stratified sample of the batch (no termination,
 // fixed iteration count, no re-centring), then the chunk length: with the chosen block
 // size, launches of a and 4a iterations give the per-iteration cost p and the fixed
 // cost o of a chunk (launch, loading and storing every instance's state, plus the
 // compaction that follows); the chunk is the shortest power of two from 256 to 8192
 // whose fixed cost is at most 2 % of its iterations -- shorter chunks drop finished
-// instances sooner, so the tail of an uneven batch is cut finer.  Instance state is
-// re-initialised afterwards by the caller.
+// instances sooner, so the tail of an uneven batch is cut finer.  Each block size is
+// tried with both SELL entry orders (one entry or a pair per lane load).  Instance
+// state is re-initialised afterwards by the caller.
 template <typename MT>
 int autotune(Ctx* ctx, BatchWork* w, const b2p_params* p, TuneCfg* best) {
     std::string key = batch_key(w, sizeof(MT) == 8 ? 0 : 1);
@@ -1161,15 +1209,18 @@ int autotune(Ctx* ctx, BatchWork* w, const b2p_params* p, TuneCfg* best) {
     tp.eps_infeasible = 0.0;
     const int trial_iters = 128;
     float best_ms = 1e30f;
-    *best = {256, 2048};
+    *best = {256, 2048, 1};
     size_t sm = smem_bytes(w, sizeof(MT));
-    auto fn = k_batch_chunk<MT>;
-    B2P_CUDA(ctx, cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-    // one trial launch of `iters` iterations over the sample with `th` threads (ms; < 0: the
-    // block size does not fit)
-    auto trial = [&](int th, int iters, float* ms) -> int {
+    for (auto f : {k_batch_chunk<MT, 1>, k_batch_chunk<MT, 2>})
+        B2P_CUDA(ctx, cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    // one trial launch of `iters` iterations over the sample with `th` threads and entry order
+    // W (ms; < 0: the block size does not fit)
+    auto trial = [&](int th, int W, int iters, float* ms) -> int {
         *ms = -1.0f;
-        int st = init_instances<MT>(ctx, w, &tp, nullptr, nullptr, nullptr);
+        auto fn = W == 2 ? k_batch_chunk<MT, 2> : k_batch_chunk<MT, 1>;
+        int st = refill_ell(ctx, w, W);
+        if (st) return st;
+        st = init_instances<MT>(ctx, w, &tp, nullptr, nullptr, nullptr);
         if (st) return st;
         int32_t cnt[2] = {0, sample};
         B2P_CUDA(ctx, cudaMemcpyAsync(w->counters.p, cnt, sizeof(cnt), cudaMemcpyHostToDevice, s));
@@ -1188,17 +1239,19 @@ int autotune(Ctx* ctx, BatchWork* w, const b2p_params* p, TuneCfg* best) {
         cudaEventElapsedTime(ms, ctx->ev0, ctx->ev1);
         return B2P_OK;
     };
-    for (int th : {128, 256, 512}) {
-        float ms = 0.0f;
-        int st = trial(th, trial_iters, &ms);
-        if (st) return st;
-        if (ms >= 0.0f && ms < best_ms) {
-            best_ms = ms;
-            best->threads = th;
+    for (int W : {1, 2})
+        for (int th : {128, 256, 512}) {
+            float ms = 0.0f;
+            int st = trial(th, W, trial_iters, &ms);
+            if (st) return st;
+            if (ms >= 0.0f && ms < best_ms) {
+                best_ms = ms;
+                best->threads = th;
+                best->w = W;
+            }
         }
-    }
     float t4 = 0.0f;
-    int st = trial(best->threads, 4 * trial_iters, &t4);
+    int st = trial(best->threads, best->w, 4 * trial_iters, &t4);
     if (st) return st;
     const double per_iter = std::max(1e-9, (double)(t4 - best_ms) / (3.0 * trial_iters));
     const double fixed = std::max(0.0, (double)best_ms - trial_iters * per_iter);
@@ -1231,10 +1284,11 @@ int batch_run(Ctx* ctx, BatchWork* w, const b2p_params* p, const double* x0_dev,
         }
     }
     w->recenter = false;  // autotune trials run without re-centring
-    TuneCfg cfg = {256, 2048};
+    TuneCfg cfg = {256, 2048, 1};
     if (w->tuned_threads[prec] > 0) {
         cfg.threads = w->tuned_threads[prec];
         cfg.chunk = w->tuned_chunk[prec];
+        cfg.w = w->tuned_w[prec];
     } else {
         if (subset) {
             ctx->err = "subset solve before a full solve of this precision";
@@ -1244,6 +1298,11 @@ int batch_run(Ctx* ctx, BatchWork* w, const b2p_params* p, const double* x0_dev,
         if (st) return st;
         w->tuned_threads[prec] = cfg.threads;
         w->tuned_chunk[prec] = cfg.chunk;
+        w->tuned_w[prec] = cfg.w;
+    }
+    {
+        int st = refill_ell(ctx, w, cfg.w);
+        if (st) return st;
     }
     // displacement buffers of the infeasibility certificates (sized for FP64, read as MT)
     if (p->eps_infeasible > 0.0) {
@@ -1292,7 +1351,7 @@ int batch_run(Ctx* ctx, BatchWork* w, const b2p_params* p, const double* x0_dev,
     int32_t cnt[2] = {0, n_act};
     B2P_CUDA(ctx, cudaMemcpyAsync(w->counters.p, cnt, sizeof(cnt), cudaMemcpyHostToDevice, s));
     size_t sm = smem_bytes(w, sizeof(MT));
-    auto fn = k_batch_chunk<MT>;
+    auto fn = cfg.w == 2 ? k_batch_chunk<MT, 2> : k_batch_chunk<MT, 1>;
     B2P_CUDA(ctx, cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
     int per_sm = 0;
     B2P_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, cfg.threads, sm));
@@ -1304,7 +1363,7 @@ int batch_run(Ctx* ctx, BatchWork* w, const b2p_params* p, const double* x0_dev,
     BArgs a1 = make_args<MT>(w, p, w->active.p);
     BArgs a2 = make_args<MT>(w, p, w->active2.p);
     // the wide form for the tail: 1024 threads, one CTA per SM
-    auto fnw = k_batch_chunk_wide<MT>;
+    auto fnw = cfg.w == 2 ? k_batch_chunk_wide<MT, 2> : k_batch_chunk_wide<MT, 1>;
     B2P_CUDA(ctx, cudaFuncSetAttribute(fnw, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
     int per_sm_w = 0;
     B2P_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_w, fnw, 1024, sm));
@@ -1449,6 +1508,7 @@ void fill_summary(b2p_result* sum, int count, bool timed_out, int64_t tot_it, in
     sum->kernel_time_ms = kms;
     sum->primal_weight = 0.0;
     sum->step_size = cfg.threads * 100000.0 + cfg.chunk;  // tuned block size * 1e5 + chunk length
+    sum->used_average = cfg.w;                              // SELL entries per lane load
 }
 
 // All instances of the batch share one shape (required by the learned warm start).
@@ -1574,13 +1634,13 @@ int b2p_batch_upload(void* p, int nmat, const int32_t* mat_m, const int32_t* mat
         rs_off[k] = (int64_t)r_sptr.size();
         for (int s0 = 0; s0 < m; s0 += 32) {
             r_sptr.push_back(r_pad);
-            r_pad += 32LL * rlen[rord[s0]];
+            r_pad += 32LL * ((rlen[rord[s0]] + 1) & ~1);  // even: both entry orders (W = 1, 2) fit
         }
         r_sptr.push_back(r_pad);
         cs_off[k] = (int64_t)c_sptr.size();
         for (int s0 = 0; s0 < n; s0 += 32) {
             c_sptr.push_back(c_pad);
-            c_pad += 32LL * clen[cord[s0]];
+            c_pad += 32LL * ((clen[cord[s0]] + 1) & ~1);
         }
         c_sptr.push_back(c_pad);
         rp_base += m + 1;
@@ -1700,10 +1760,10 @@ int b2p_batch_upload(void* p, int nmat, const int32_t* mat_m, const int32_t* mat
     k_batch_power<<<gmat, 256, 0, s>>>(nmat, w->mat_m.p, w->mat_n.p, w->mat_row_off.p, w->mat_col_off.p, w->rowptr.p,
                                         w->colidx.p, w->sv64.p, w->t_rowptr.p, w->t_colidx.p, w->stv64.p, w->pv.p,
                                         w->pu.p, 0.998, w->mat_eta.p);
-    k_fill_ell<<<gmat, 256, 0, s>>>(nmat, w->mat_m.p, w->mat_row_off.p, w->mat_col_off.p, w->mat_rs_off.p, w->r_sptr.p,
+    k_fill_ell<<<gmat, 256, 0, s>>>(1, nmat, w->mat_m.p, w->mat_row_off.p, w->mat_col_off.p, w->mat_rs_off.p, w->r_sptr.p,
                                      w->rowptr.p, w->colidx.p, w->sv64.p, w->sv32.p, w->r_eidx.p, w->r_ev64.p,
                                      w->r_ev32.p);
-    k_fill_ell<<<gmat, 256, 0, s>>>(nmat, w->mat_n.p, w->mat_col_off.p, w->mat_row_off.p, w->mat_cs_off.p, w->c_sptr.p,
+    k_fill_ell<<<gmat, 256, 0, s>>>(1, nmat, w->mat_n.p, w->mat_col_off.p, w->mat_row_off.p, w->mat_cs_off.p, w->c_sptr.p,
                                      w->t_rowptr.p, w->t_colidx.p, w->stv64.p, w->stv32.p, w->c_eidx.p, w->c_ev64.p,
                                      w->c_ev32.p);
     B2P_LAUNCH(ctx);
