@@ -3,7 +3,7 @@
 // GEMM: C[M,N] (FP32) = A[M,K] . B[N,K]^T with A, B BF16 row-major (both
 // K-major, "TN").  One CTA computes one 128 x 128 output tile:
 //   * warp 0, one elected thread: TMA producer -- cp.async.bulk.tensor.2d loads of
-//     128 x 64 BF16 tiles of A and B (128-byte swizzle) into a 4-stage shared
+//     128 x 64 BF16 tiles of A and B (128-byte swizzle) into a 3-stage shared
 //     memory ring, completion signalled on per-stage mbarriers (expect_tx);
 //   * warp 1, one elected thread: issues tcgen05.mma.cta_group::1.kind::f16
 //     (M = 128, N = 128, K = 16 per instruction, BF16 x BF16 -> FP32) reading
@@ -159,13 +159,16 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
     for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
 
-constexpr int GBM = 128, GBN = 128, GBK = 64, GSTAGES = 4;
+// Three stages (about 100 KB of shared memory) let two CTAs share an SM -- and its TMEM, 128
+// columns each -- so one CTA's epilogue overlaps the other's main loop and a 256 x 10,008
+// output fits in one wave.
+constexpr int GBM = 128, GBN = 128, GBK = 64, GSTAGES = 3;
 constexpr int GTILE_A = GBM * GBK * 2, GTILE_B = GBN * GBK * 2;
 constexpr size_t GEMM_SMEM = 1024 + GSTAGES * (GTILE_A + GTILE_B) + 256;
 
 // C[M,N] = A[M,K] . B[N,K]^T ; A, B through tensor maps; C FP32 row-major, ldc elements.
 // Split-K: CTA z of gridDim.z sums k-blocks [z kbs, (z + 1) kbs) into C + z split_stride.
-__global__ void __launch_bounds__(128, 1)
+__global__ void __launch_bounds__(128, 2)
 k_gemm_tn_bf16(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, float* __restrict__ C,
                int M, int N, int K, int ldc, int kbs, size_t split_stride, int* err) {
     extern __shared__ uint8_t smem_raw[];
