@@ -121,11 +121,12 @@ def profile_learned(args):
         ws.fit(n_train=1024, label_eps=1e-6, epochs=20, max_iterations=100000)
         b2p.warmstart.upload_family(ctx, fam, P)
         F = P.astype(np.float32)
+        judge = dict(eps=args.eps, eps_objective=args.eps_objective)
         legs = {
-            "learned": lambda it: ctx.batch_solve_learned(F, precision="fp32", eps=args.eps, max_iterations=it,
-                                                          outputs=False),
-            "mixed_cold": lambda it: ctx.batch_solve(precision="fp32", eps=args.eps, max_iterations=it, outputs=False),
-            "fp64_cold": lambda it: ctx.batch_solve(precision="fp64", eps=args.eps, max_iterations=it, outputs=False),
+            "learned": lambda it: ctx.batch_solve_learned(F, precision="fp32", max_iterations=it, outputs=False,
+                                                          **judge),
+            "mixed_cold": lambda it: ctx.batch_solve(precision="fp32", max_iterations=it, outputs=False, **judge),
+            "fp64_cold": lambda it: ctx.batch_solve(precision="fp64", max_iterations=it, outputs=False, **judge),
         }
         for fn in legs.values():
             fn(2048)
