@@ -50,8 +50,8 @@ METRIC = "LPs/sec to 1e-6 rel KKT"
 # Seconds of each part of the refinery_learned run on one B200 (2,000 held-out
 # instances; labels to 1e-8, legs to 1e-6 relative KKT with the answer's objective
 # within 1e-6), used to plan the run's wall time from its leg counts.
-LEARNED_LEG_S = {"start": 30.0, "label_per_instance": 0.0144, "epoch": 0.044, "warmup_step": 2.0,
-                 "learned": 53.0, "mixed_cold": 57.0, "fp64_cold": 93.0, "e2e": 54.0, "cpu_sample": 15.0}
+LEARNED_LEG_S = {"start": 20.0, "label_per_instance": 0.0156, "epoch": 0.031, "warmup_step": 1.5,
+                 "learned": 29.2, "mixed_cold": 30.3, "fp64_cold": 45.9, "e2e": 29.4, "cpu_sample": 12.0}
 
 
 def metric_for(args):

@@ -50,3 +50,18 @@ def test_reference_arm_json_line():
     assert line["impl"] == "reference" and line["value"] > 0
     assert line["cpu_baseline"]["kind"] in ("reference", "port") and line["cpu_baseline"]["cores"] >= 1
     assert line["e2e"]["h2d_bytes_per_step"] == 0 and line["e2e"]["value"] == line["value"]
+
+
+def test_learned_plan_fits_driver_command(monkeypatch):
+    """The fixed driver command (--steps 20 --warmup 5) on the full configuration
+    (20k labels, 600 epochs, 2k held-out) plans within 1,200 s: only the value leg
+    repeats --steps times, the comparison and e2e legs run their own small counts."""
+    import bench
+    a = _parse(monkeypatch, "--steps", "20", "--warmup", "5")
+    assert a.train_count == 20000 and a.epochs == 600 and a.heldout == 2000
+    assert a.compare_steps == 1 and a.e2e_steps == 1
+    plan = bench.planned_wall_s(a)
+    assert plan <= 1200.0, plan
+    # the value leg is what grows with --steps
+    b = _parse(monkeypatch, "--steps", "21", "--warmup", "5")
+    assert bench.planned_wall_s(b) - plan == pytest.approx(bench.LEARNED_LEG_S["learned"])
