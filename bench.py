@@ -47,6 +47,19 @@ HALPERN_ITERS = {"block_angular": 6784, "random_sparse": 5056, "refinery_learned
 
 METRIC = "LPs/sec to 1e-6 rel KKT"
 
+# Copy bandwidth (STREAM-style) and sustained BF16 GEMM throughput (cuBLAS loop under the
+# power cap) measured on B200 in an earlier run; the roofline denominators when no
+# MEASURED_PEAKS.json sits beside this file.
+EARLIER_PEAKS = {"hbm_gbs": 6558.7, "bf16_tflops_sustained": 1371.5}
+
+
+def peaks():
+    """(measured peaks, label of their source)."""
+    f = ROOT / "MEASURED_PEAKS.json"
+    if f.exists():
+        return json.loads(f.read_text()), "MEASURED_PEAKS.json (of measured)"
+    return dict(EARLIER_PEAKS), "B200 copy / BF16 GEMM measured in an earlier run; MEASURED_PEAKS.json absent (of measured)"
+
 # Seconds of each part of the refinery_learned run on one B200 (2,000 held-out
 # instances; labels to 1e-8, legs to 1e-6 relative KKT with the answer's objective
 # within 1e-6), used to plan the run's wall time from its leg counts.
@@ -508,8 +521,8 @@ def run_batch_workload(args):
     # matrices and vectors the resident instances stream exceed L2, else L2
     per_iter = np.array([12.0 * s_.nnz + 24.0 * s_.n + 16.0 * s_.m for s_ in stds])
     alg = float((per_inst_iters * per_iter).sum())
-    peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
-    peak = peaks.get("hbm_gbs", 6650.0)
+    pk, pk_src = peaks()
+    peak = pk["hbm_gbs"]
     achieved = alg / (kern_ms / 1e3) / 1e9
     resident = 2 * 148  # two CTAs per SM, one instance each
     vec = np.array([24.0 * s_.n + 16.0 * s_.m for s_ in stds])
@@ -520,8 +533,7 @@ def run_batch_workload(args):
     roofline = {"bound": bound, "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "traffic": None, "kernel": "k_batch_chunk<float>",
                 "algorithmic_bytes_per_instance_iteration_mean": float(per_iter.mean()),
-                "resident_working_set_bytes": hot,
-                "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if peaks else "fallback 6650 (of fallback)"}
+                "resident_working_set_bytes": hot, "peak_source": "hbm_gbs: " + pk_src}
     cpu = None
     if rank == 0 and world == 1 and "fp64" in res:
         cpu = cpu_reference_sample(lps[0], 2000, int(res["fp64"]["iterations_mean"]))
@@ -687,8 +699,8 @@ def run_learned_workload(args):
     # the on-chip one; the DRAM share comes from the committed ncu capture.
     nnz = int(fam.rowptr[-1])
     per_iter = 12 * nnz + 24 * fam.n + 16 * fam.m
-    peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
-    peak = peaks.get("hbm_gbs", 6650.0)
+    pk, pk_src = peaks()
+    peak = pk["hbm_gbs"]
     achieved = it_total * per_iter / (kern_ms / 1e3) / 1e9
     prof = read_profile(ROOT / "profiles" / "batch_chunk_refinery_planning.txt")
     roofline = {"bound": "l2", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
@@ -700,8 +712,7 @@ def run_learned_workload(args):
                 "lts_throughput_pct": prof.get("lts_throughput_pct"),
                 "kernel": "k_batch_chunk<float> (SELL, learned leg)",
                 "algorithmic_bytes_per_instance_iteration": per_iter,
-                "peak_source": ("MEASURED_PEAKS.json hbm_gbs (of measured); no measured L2 peak exists, so the "
-                                "fraction is against HBM" if peaks else "fallback 6650 (of fallback)"),
+                "peak_source": "hbm_gbs: " + pk_src + "; no measured L2 peak exists, so the fraction is against HBM",
                 "note": "12 B per nonzero (FP32 value + 16-bit index, both orientations), 24 B per column, 16 B per "
                         "row; bound 'l2': the shared matrix and the instances' vectors stay in L2 / shared memory "
                         "(ncu: DRAM carries dram_frac of these bytes)"}
@@ -710,11 +721,10 @@ def run_learned_workload(args):
     # training time, against the sustained BF16 peak
     hid, outp = 1024, (fam.n + fam.m + 1 + 7) // 8 * 8
     flop = (4.0 * fam.N_PARAM * hid + 6.0 * hid * hid + 6.0 * hid * outp) * args.train_count * args.epochs
-    bf16 = peaks.get("bf16_tflops_sustained") or peaks.get("bf16_tflops") or 1400.0
+    bf16 = pk.get("bf16_tflops_sustained") or pk.get("bf16_tflops")
     fit["train_tflops"] = flop / max(fit["train_s"], 1e-9) / 1e12
     fit["train_frac_of_bf16_sustained"] = fit["train_tflops"] / bf16
-    fit["train_peak_source"] = ("MEASURED_PEAKS.json (of measured)" if peaks.get("bf16_tflops_sustained")
-                                else "fallback 1400 TFLOP/s sustained BF16 (of fallback)")
+    fit["train_peak_source"] = "bf16_tflops_sustained: " + pk_src
     fit["train_flop"] = flop
     cpu = None
     if rank == 0 and world == 1:
@@ -889,8 +899,8 @@ def main():
     # after a (capped) mixed solve has set up the tuned kernels
     ctx.solve(precision="fp32", **warm)
     kt = ctx.kernel_timing(reps=20, precision="fp32", **common)
-    peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
-    peak = peaks.get("hbm_gbs", 6650.0)
+    pk, pk_src = peaks()
+    peak = pk["hbm_gbs"]
     dom = "primal" if kt["primal_ms"] >= kt["dual_ms"] else "dual"
     achieved = kt[f"{dom}_bytes"] / (kt[f"{dom}_ms"] / 1e3) / 1e9
     traffic = None
@@ -904,7 +914,7 @@ def main():
                 "algorithmic_bytes": kt[f"{dom}_bytes"],
                 "iteration": {"ms": kt["primal_ms"] + kt["dual_ms"],
                               "GB/s": (kt["primal_bytes"] + kt["dual_bytes"]) / ((kt["primal_ms"] + kt["dual_ms"]) / 1e3) / 1e9},
-                "peak_source": "MEASURED_PEAKS.json hbm_gbs (burst copy) of measured" if peaks else "fallback 6650"}
+                "peak_source": "hbm_gbs: " + pk_src}
     # end to end through the public API: pinned host buffers -> upload (H2D + transpose) -> solve -> x, y to host
     pin = {k: torch.from_numpy(np.ascontiguousarray(getattr(std, k))).pin_memory()
            for k in ("rowptr", "colidx", "vals", "b", "c", "lb", "ub", "is_eq")}

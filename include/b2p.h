@@ -273,7 +273,12 @@ int b2p_batch_upload(void* ctx, int nmat, const int32_t* mat_m, const int32_t* m
 /* Solve all instances with the Halpern engine.  x0/y0 optional warm starts
  * (concatenated like c / b), omega0 optional per-instance primal weights.
  * Outputs (optional): per-instance status, iterations, rel KKT and final primal
- * weight; concatenated x, y. */
+ * weight; concatenated x, y.  The summary reports the autotuned kernel shape:
+ * step_size = CTA size * 1e5 + chunk length (iterations per persistent launch),
+ * used_average = 10 * instances per CTA (2: the paired form, batches whose
+ * instances share one matrix) + SELL entries per lane load.  The shape is tuned
+ * once per batch signature and cached in the file B2P_AUTOTUNE_CACHE (default
+ * ~/.cache/b2p_autotune.txt); B2P_BATCH_SHAPE="threads,w,ni" pins it. */
 int b2p_batch_solve(void* ctx, const b2p_params* params, const double* x0, const double* y0, const double* omega0,
                     int32_t* status_out, int64_t* iters_out, double* kkt_out, double* omega_out, double* x_out,
                     double* y_out, b2p_result* summary);

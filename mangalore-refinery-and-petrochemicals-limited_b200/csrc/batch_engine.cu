@@ -53,6 +53,7 @@
 #include <algorithm>
 #include <type_traits>
 #include <cmath>
+#include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <fstream>
@@ -115,6 +116,7 @@ struct BatchWork {
     int tuned_threads[2] = {0, 0};  // block size per precision (0 = not tuned yet)
     int tuned_chunk[2] = {2048, 2048};  // iterations per chunk launch per precision
     int tuned_w[2] = {1, 1};        // SELL entry order per precision
+    int tuned_ni[2] = {1, 1};       // instances per CTA per precision (2: paired form)
     int ell_w = 1;                  // entry order the SELL copies hold now
     DBuf<int32_t> list;             // instances re-initialised by a subset solve
     // active-instance trace of the last solve: host time (ms from the first graph launch of
@@ -257,6 +259,75 @@ __device__ __forceinline__ MT ell_dot(const MT* __restrict__ v, const uint16_t* 
     return s;
 }
 
+// ell_dot for two instances of one matrix: every value and index load of the slice
+// feeds a gather from each instance's operand (g0, g1) and two independent sums, each
+// in the entry order of ell_dot (the same results as two ell_dot calls).
+template <typename MT, int W>
+__device__ __forceinline__ void ell_dot2(const MT* __restrict__ v, const uint16_t* __restrict__ ix, int len,
+                                         const MT* __restrict__ g0, const MT* __restrict__ g1, MT& s0, MT& s1) {
+    constexpr int B = sizeof(MT) == 4 ? 8 : 4;
+    MT a0 = (MT)0, a1 = (MT)0;
+    if constexpr (W == 1) {
+        for (int q = 0; q < len; q += B) {
+            MT vv[B];
+            unsigned ii[B];
+#pragma unroll
+            for (int u = 0; u < B; ++u) {
+                const bool h = q + u < len;
+                vv[u] = h ? v[(q + u) * 32] : (MT)0;
+                ii[u] = h ? (unsigned)ix[(q + u) * 32] : 0u;
+            }
+#pragma unroll
+            for (int u = 0; u < B; ++u)
+                if (q + u < len) {
+                    a0 += vv[u] * g0[ii[u]];
+                    a1 += vv[u] * g1[ii[u]];
+                }
+        }
+    } else {
+        typedef typename std::conditional<sizeof(MT) == 4, float2, double2>::type MT2;
+        constexpr int P = B / 2;
+        const int np = len >> 1;
+        for (int t = 0; t < np; t += P) {
+            MT2 vv[P];
+            unsigned ii[P];
+#pragma unroll
+            for (int u = 0; u < P; ++u) {
+                const bool h = t + u < np;
+                vv[u] = h ? *reinterpret_cast<const MT2*>(v + (t + u) * 64) : MT2{(MT)0, (MT)0};
+                ii[u] = h ? *reinterpret_cast<const unsigned*>(ix + (t + u) * 64) : 0u;
+            }
+#pragma unroll
+            for (int u = 0; u < P; ++u)
+                if (t + u < np) {
+                    const unsigned lo = ii[u] & 0xFFFFu, hi = ii[u] >> 16;
+                    a0 += vv[u].x * g0[lo];
+                    a1 += vv[u].x * g1[lo];
+                    a0 += vv[u].y * g0[hi];
+                    a1 += vv[u].y * g1[hi];
+                }
+        }
+    }
+    s0 = a0;
+    s1 = a1;
+}
+
+// Entries of a CTA's slice table (column slices, then row slices; even, so what follows
+// it in shared memory stays 16-byte aligned).
+__host__ __device__ __forceinline__ int slice_tab_len(int nrs, int ncs) { return (nrs + ncs + 1) & ~1; }
+
+// The slice table of one matrix in shared memory, built when a CTA takes an instance:
+// per slice {first entry, entries per lane}.  The iterations then read one 8-byte shared
+// word per slice instead of two slice pointers from L2 in front of every value load.
+// Entry offsets fit 32 bits (the upload refuses batches whose SELL copies do not).
+__device__ __forceinline__ void fill_slice_tab(int2* tab, const int64_t* __restrict__ csp, int ncs,
+                                               const int64_t* __restrict__ rsp, int nrs) {
+    for (int i = threadIdx.x; i < ncs; i += blockDim.x)
+        tab[i] = make_int2((int)csp[i], (int)((csp[i + 1] - csp[i]) >> 5));
+    for (int i = threadIdx.x; i < nrs; i += blockDim.x)
+        tab[ncs + i] = make_int2((int)rsp[i], (int)((rsp[i + 1] - rsp[i]) >> 5));
+}
+
 // Slice of round r for warp w of nw: rounds alternate the direction in which the
 // (length-sorted) slices are dealt, w then nw - 1 - w, so every warp's share of long
 // and short slices is even.  Increasing in r for a fixed warp.
@@ -317,6 +388,43 @@ __device__ void rebuild_shifted(const BArgs& a, int m, int n, int64_t ro, int64_
     }
 }
 
+// Restart of one instance after its check decided so, by every thread of the owning
+// CTA (ys: its dual iterate in shared memory): z <- anchor <- T(z), or, re-centred,
+// T(z) becomes the new FP64 centre and the shifted problem is rebuilt around it.
+template <typename MT>
+__device__ __forceinline__ void restart_instance(const BArgs& a, int m, int n, int64_t ro, int64_t co, int64_t xo,
+                                              int64_t yo, MT* ys) {
+    const int tid = threadIdx.x, nt = blockDim.x;
+    ColP<MT>* colp = (ColP<MT>*)a.colp;
+    RowP<MT>* rowp = (RowP<MT>*)a.rowp;
+    MT *xg = (MT*)a.x, *xtg = (MT*)a.xt, *ytg = (MT*)a.yt;
+    if (!a.recenter) {
+        for (int j = tid; j < n; j += nt) {
+            const MT v = xtg[xo + j];
+            xg[xo + j] = v;
+            colp[xo + j].a = v;
+        }
+        for (int i = tid; i < m; i += nt) {
+            const MT v = ytg[yo + i];
+            ys[i] = v;
+            rowp[yo + i].a = v;
+        }
+    } else {
+        for (int j = tid; j < n; j += nt) {
+            a.xbar[xo + j] += a.dc[co + j] * (double)xtg[xo + j];
+            xg[xo + j] = (MT)0;
+            xtg[xo + j] = (MT)0;
+        }
+        for (int i = tid; i < m; i += nt) {
+            a.ybar[yo + i] += a.dr[ro + i] * (double)ytg[yo + i];
+            ys[i] = (MT)0;
+            ytg[yo + i] = (MT)0;
+        }
+        __syncthreads();
+        rebuild_shifted<MT>(a, m, n, ro, co, xo, yo);
+    }
+}
+
 // Restart-check iteration of one instance, run by every thread of the owning CTA
 // after T(z) (xt, yt) and, with certificates on, the displacement (dx, dy) are in
 // global memory: the FP64 KKT of T(z) on the original instance, the objective-error
@@ -360,6 +468,7 @@ __device__ __noinline__ void check_instance(const BArgs& a, int inst, int m, int
             const double yv = (a.recenter ? a.ybar[yo + i] : 0.0) + dri * (double)ytg[yo + i];
             kk2[1] += a.b[yo + i] * yv;
             kk2[5] += fabs(yv) * fabs(rp);
+            if (!a.is_eq[yo + i] && yv < 0.0) kk2[2] += yv * yv;  // y >= 0 on <= rows (dual residual)
         }
     }
     for (int base = 0; base < n; base += cgroups) {
@@ -529,8 +638,10 @@ __device__ __forceinline__ void batch_chunk_body(const BArgs& a, int chunk) {
         const int64_t* csp = a.c_sptr + a.mat_cs_off[mat];
         const int nrs = (m + 31) >> 5, ncs = (n + 31) >> 5;
         const double eta = a.mat_eta[mat];
-        MT* ys = (MT*)smem_raw;
+        int2* tab = (int2*)smem_raw;  // column slices, then row slices
+        MT* ys = (MT*)(tab + slice_tab_len(nrs, ncs));
         MT* xhs = ys + ((m + 3) & ~3);
+        fill_slice_tab(tab, csp, ncs, rsp, nrs);
         if (tid == 0) sc = a.ictrl[inst];
         for (int i = tid; i < m; i += nt) ys[i] = yg[yo + i];
         __syncthreads();
@@ -557,8 +668,8 @@ __device__ __forceinline__ void batch_chunk_body(const BArgs& a, int chunk) {
                     p = colp[xo + j];
                     x0 = xg[xo + j];
                 }
-                const int64_t p0 = csp[sl];
-                const int len = (int)((csp[sl + 1] - p0) >> 5);
+                const int2 t = tab[sl];
+                const int p0 = t.x, len = t.y;
                 const MT s = len <= kLongSlice
                                  ? ell_dot<MT, W>(cev + p0 + W * lane, a.c_eidx + p0 + W * lane, len, ys)
                                  : long_slice_dot<MT>(stv, a.t_rowptr, a.t_colidx, co + (sl << 5), min(32, n - (sl << 5)),
@@ -586,8 +697,8 @@ __device__ __forceinline__ void batch_chunk_body(const BArgs& a, int chunk) {
                 const bool valid = i < m;
                 RowP<MT> p;
                 if (valid) p = rowp[yo + i];
-                const int64_t p0 = rsp[sl];
-                const int len = (int)((rsp[sl + 1] - p0) >> 5);
+                const int2 t = tab[ncs + sl];
+                const int p0 = t.x, len = t.y;
                 const MT s = len <= kLongSlice
                                  ? ell_dot<MT, W>(rev + p0 + W * lane, a.r_eidx + p0 + W * lane, len, xhs)
                                  : long_slice_dot<MT>(sv, a.rowptr, a.colidx, ro + (sl << 5), min(32, m - (sl << 5)),
@@ -648,31 +759,7 @@ __device__ __forceinline__ void batch_chunk_body(const BArgs& a, int chunk) {
             if (s_flags[1]) {
                 kk = 0;
                 first = true;
-                if (!a.recenter) {  // restart: z <- anchor <- T(z)
-                    for (int j = tid; j < n; j += nt) {
-                        const MT v = xtg[xo + j];
-                        xg[xo + j] = v;
-                        colp[xo + j].a = v;
-                    }
-                    for (int i = tid; i < m; i += nt) {
-                        const MT v = ytg[yo + i];
-                        ys[i] = v;
-                        rowp[yo + i].a = v;
-                    }
-                } else {  // restart at T(z) as the new FP64 centre
-                    for (int j = tid; j < n; j += nt) {
-                        a.xbar[xo + j] += a.dc[co + j] * (double)xtg[xo + j];
-                        xg[xo + j] = (MT)0;
-                        xtg[xo + j] = (MT)0;
-                    }
-                    for (int i = tid; i < m; i += nt) {
-                        a.ybar[yo + i] += a.dr[ro + i] * (double)ytg[yo + i];
-                        ys[i] = (MT)0;
-                        ytg[yo + i] = (MT)0;
-                    }
-                    __syncthreads();
-                    rebuild_shifted<MT>(a, m, n, ro, co, xo, yo);
-                }
+                restart_instance<MT>(a, m, n, ro, co, xo, yo, ys);
             }
             __syncthreads();
         }
@@ -696,6 +783,269 @@ __global__ void __launch_bounds__(512, 2) k_batch_chunk(const __grid_constant__ 
 template <typename MT, int W>
 __global__ void __launch_bounds__(1024, 1) k_batch_chunk_wide(const __grid_constant__ BArgs a, int chunk) {
     batch_chunk_body<MT, W>(a, chunk);
+}
+
+// Paired form of the chunk kernel for a batch whose instances all share one matrix
+// (a parametric family): a CTA takes two consecutive entries of the active list and
+// iterates both instances in lockstep, so every SELL value and index load of the
+// shared matrix feeds both instances' gathers (ell_dot2) -- the matrix bytes per
+// instance-iteration halve and each warp carries two independent sums per load.
+// Shared memory holds y and xh of both instances.  Per instance everything is as in
+// batch_chunk_body, with the same thread-to-column/row assignment and arithmetic, so
+// the iterates and decisions are those of the single form bit for bit.  An instance
+// that finishes leaves its partner to iterate alone (single gathers) until the chunk
+// ends; the compaction between chunks re-pairs the survivors.
+template <typename MT, int W>
+__device__ __forceinline__ void batch_pair_body(const BArgs& a, int chunk) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ double red[32 * 7];
+    __shared__ InstCtrl sc[2];
+    __shared__ int s_q;
+    __shared__ int s_flags[2][2];  // per instance -- 0: done, 1: restart
+    const int tid = threadIdx.x, nt = blockDim.x;
+    const int lane = tid & 31, warp = tid >> 5, nwarps = nt >> 5;
+    const MT* sv = (const MT*)a.sv;
+    const MT* stv = (const MT*)a.stv;
+    const MT* rev = (const MT*)a.r_ev;
+    const MT* cev = (const MT*)a.c_ev;
+    ColP<MT>* colp = (ColP<MT>*)a.colp;
+    RowP<MT>* rowp = (RowP<MT>*)a.rowp;
+    MT *xg = (MT*)a.x, *xtg = (MT*)a.xt, *yg = (MT*)a.y, *ytg = (MT*)a.yt;
+    MT *dxg = (MT*)a.dx, *dyg = (MT*)a.dy;
+    const bool rays = a.eps_inf > 0.0;
+    const int active_count = a.counters[1];
+    const MT rho = (MT)a.rho, one_rho = (MT)(1.0 + a.rho);
+    // the one matrix of the batch
+    const int m = a.mat_m[0], n = a.mat_n[0];
+    const int64_t ro = a.mat_row_off[0], co = a.mat_col_off[0];
+    const int64_t* rsp = a.r_sptr + a.mat_rs_off[0];
+    const int64_t* csp = a.c_sptr + a.mat_cs_off[0];
+    const int nrs = (m + 31) >> 5, ncs = (n + 31) >> 5;
+    const double eta = a.mat_eta[0];
+    const int m4 = (m + 3) & ~3, stride = m4 + ((n + 3) & ~3);
+    int2* tab = (int2*)smem_raw;  // column slices, then row slices (built once: one matrix)
+    MT* ysb[2] = {(MT*)(tab + slice_tab_len(nrs, ncs)), (MT*)(tab + slice_tab_len(nrs, ncs)) + stride};
+    MT* xhb[2] = {ysb[0] + m4, ysb[1] + m4};
+    fill_slice_tab(tab, csp, ncs, rsp, nrs);
+    while (true) {
+        if (tid == 0) s_q = atomicAdd(&a.counters[0], 2);
+        __syncthreads();
+        const int q = s_q;
+        if (q >= active_count) break;
+        const bool has2 = q + 1 < active_count;
+        int inst[2];
+        inst[0] = a.active[q];
+        inst[1] = has2 ? a.active[q + 1] : inst[0];
+        bool live[2] = {true, has2};
+        int64_t xo[2], yo[2];
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+            xo[k] = a.x_off[inst[k]];
+            yo[k] = a.y_off[inst[k]];
+        }
+        if (tid == 0) sc[0] = a.ictrl[inst[0]];
+        if (tid == 1 && has2) sc[1] = a.ictrl[inst[1]];
+#pragma unroll
+        for (int k = 0; k < 2; ++k)
+            if (live[k])
+                for (int i = tid; i < m; i += nt) ysb[k][i] = yg[yo[k] + i];
+        __syncthreads();
+        long long kk[2], total[2];
+        bool first[2];
+        double om[2];
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+            const int src = live[k] ? k : 0;
+            kk[k] = sc[src].k;
+            total[k] = sc[src].total;
+            first[k] = sc[src].first != 0;
+            om[k] = sc[src].omega;
+        }
+        __syncthreads();  // every thread holds its copies before thread 0 writes sc again
+        for (int it = 0; it < chunk && (live[0] || live[1]); ++it) {
+            bool check[2], stats[2];
+            MT tau[2], sigma[2], wk[2], wa[2];
+#pragma unroll
+            for (int k = 0; k < 2; ++k) {
+                check[k] = live[k] && ((total[k] + 1) % a.K) == 0;
+                stats[k] = live[k] && (first[k] || check[k]);
+                tau[k] = (MT)(eta / om[k]);
+                sigma[k] = (MT)(eta * om[k]);
+                wk[k] = (MT)((kk[k] + 1.0) / (kk[k] + 2.0));
+                wa[k] = (MT)(1.0 / (kk[k] + 2.0));
+            }
+            const bool both = live[0] && live[1];
+            const bool solo1 = !live[0];  // the one live instance when not both
+            const MT* ys_solo = solo1 ? ysb[1] : ysb[0];
+            const MT* xh_solo = solo1 ? xhb[1] : xhb[0];
+            double acc[2][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}};
+            // ---- primal phase
+            for (int r = 0, sl = warp; sl < ncs; ++r, sl = snake_slice(r, warp, nwarps)) {
+                const int j = (sl << 5) + lane;
+                const bool valid = j < n;
+                ColP<MT> p[2];
+                MT x0[2] = {(MT)0, (MT)0};
+#pragma unroll
+                for (int k = 0; k < 2; ++k)
+                    if (valid && live[k]) {
+                        p[k] = colp[xo[k] + j];
+                        x0[k] = xg[xo[k] + j];
+                    }
+                const int2 tb = tab[sl];
+                const int p0 = tb.x, len = tb.y;
+                MT s[2] = {(MT)0, (MT)0};
+                if (len <= kLongSlice) {
+                    if (both)
+                        ell_dot2<MT, W>(cev + p0 + W * lane, a.c_eidx + p0 + W * lane, len, ysb[0], ysb[1], s[0], s[1]);
+                    else {
+                        const MT t = ell_dot<MT, W>(cev + p0 + W * lane, a.c_eidx + p0 + W * lane, len, ys_solo);
+                        s[0] = solo1 ? (MT)0 : t;
+                        s[1] = solo1 ? t : (MT)0;
+                    }
+                } else {
+#pragma unroll
+                    for (int k = 0; k < 2; ++k)
+                        if (live[k])
+                            s[k] = long_slice_dot<MT>(stv, a.t_rowptr, a.t_colidx, co + (sl << 5),
+                                                      min(32, n - (sl << 5)), ro, ysb[k], lane);
+                }
+#pragma unroll
+                for (int k = 0; k < 2; ++k)
+                    if (valid && live[k]) {
+                        const MT xt = clampT(x0[k] - tau[k] * (p[k].c + s[k]), p[k].l, p[k].u);
+                        xhb[k][j] = (MT)2 * xt - x0[k];
+                        xg[xo[k] + j] = wk[k] * (one_rho * xt - rho * x0[k]) + wa[k] * p[k].a;
+                        if (stats[k]) {
+                            const double d = (double)x0[k] - (double)xt;
+                            acc[k][0] += d * d;
+                        }
+                        if (check[k]) {
+                            xtg[xo[k] + j] = xt;
+                            if (rays) dxg[xo[k] + j] = xt - x0[k];
+                            const double e = (double)xt - (double)p[k].a;
+                            acc[k][1] += e * e;
+                        }
+                    }
+            }
+            __syncthreads();
+            // ---- dual phase
+            for (int r = 0, sl = warp; sl < nrs; ++r, sl = snake_slice(r, warp, nwarps)) {
+                const int i = (sl << 5) + lane;
+                const bool valid = i < m;
+                RowP<MT> p[2];
+#pragma unroll
+                for (int k = 0; k < 2; ++k)
+                    if (valid && live[k]) p[k] = rowp[yo[k] + i];
+                const int2 tb = tab[ncs + sl];
+                const int p0 = tb.x, len = tb.y;
+                MT s[2] = {(MT)0, (MT)0};
+                if (len <= kLongSlice) {
+                    if (both)
+                        ell_dot2<MT, W>(rev + p0 + W * lane, a.r_eidx + p0 + W * lane, len, xhb[0], xhb[1], s[0], s[1]);
+                    else {
+                        const MT t = ell_dot<MT, W>(rev + p0 + W * lane, a.r_eidx + p0 + W * lane, len, xh_solo);
+                        s[0] = solo1 ? (MT)0 : t;
+                        s[1] = solo1 ? t : (MT)0;
+                    }
+                } else {
+#pragma unroll
+                    for (int k = 0; k < 2; ++k)
+                        if (live[k])
+                            s[k] = long_slice_dot<MT>(sv, a.rowptr, a.colidx, ro + (sl << 5), min(32, m - (sl << 5)),
+                                                      co, xhb[k], lane);
+                }
+#pragma unroll
+                for (int k = 0; k < 2; ++k)
+                    if (valid && live[k]) {
+                        const MT y0 = ysb[k][i];
+                        MT yt = y0 + sigma[k] * (s[k] - p[k].b);
+                        if (yt < p[k].lo) yt = p[k].lo;  // NaN stays NaN
+                        ysb[k][i] = wk[k] * (one_rho * yt - rho * y0) + wa[k] * p[k].a;
+                        if (stats[k]) {
+                            const double d = (double)y0 - (double)yt;
+                            acc[k][2] += d * d;
+                        }
+                        if (check[k]) {
+                            ytg[yo[k] + i] = yt;
+                            if (rays) {
+                                MT d = yt - y0;
+                                if (p[k].lo != (MT)(-INFINITY) && d < (MT)0) d = (MT)0;
+                                dyg[yo[k] + i] = d;
+                            }
+                            const double e = (double)yt - (double)p[k].a;
+                            acc[k][3] += e * e;
+                        }
+                    }
+            }
+#pragma unroll
+            for (int k = 0; k < 2; ++k)
+                if (live[k]) {
+                    kk[k] += 1;
+                    total[k] += 1;
+                }
+            if (!stats[0] && !stats[1]) {
+                __syncthreads();
+                continue;
+            }
+            // ---- per instance: restart reference residual, or the check and its decisions
+#pragma unroll
+            for (int k = 0; k < 2; ++k) {
+                if (!stats[k]) continue;
+                block_sums<4>(acc[k], red);
+                const bool was_first = first[k];
+                first[k] = false;
+                if (!check[k]) {
+                    if (tid == 0) {
+                        sc[k].r0 = sqrt(om[k] * acc[k][0] + acc[k][2] / om[k]);
+                        sc[k].rprev = sc[k].r0;
+                    }
+                    __syncthreads();
+                    continue;
+                }
+                double r_now = 0, dxa = 0, dya = 0;
+                if (tid == 0) {
+                    r_now = sqrt(om[k] * acc[k][0] + acc[k][2] / om[k]);
+                    if (was_first) {
+                        sc[k].r0 = r_now;
+                        sc[k].rprev = r_now;
+                    }
+                    dxa = sqrt(acc[k][1]);
+                    dya = sqrt(acc[k][3]);
+                }
+                __syncthreads();
+                check_instance<MT>(a, inst[k], m, n, ro, co, xo[k], yo[k], total[k], kk[k], om[k], r_now, dxa, dya,
+                                   sc[k], s_flags[k], red);
+                __syncthreads();
+                live[k] = s_flags[k][0] == 0;
+                om[k] = sc[k].omega;
+                if (s_flags[k][1]) {
+                    kk[k] = 0;
+                    first[k] = true;
+                    restart_instance<MT>(a, m, n, ro, co, xo[k], yo[k], ysb[k]);
+                }
+                __syncthreads();
+            }
+        }
+        // store the dual iterates and the control blocks
+#pragma unroll
+        for (int k = 0; k < 2; ++k)
+            if (k == 0 || has2)
+                for (int i = tid; i < m; i += nt) yg[yo[k] + i] = ysb[k][i];
+#pragma unroll
+        for (int k = 0; k < 2; ++k)
+            if (tid == k && (k == 0 || has2)) {
+                sc[k].k = kk[k];
+                sc[k].total = total[k];
+                sc[k].first = first[k] ? 1 : 0;
+                a.ictrl[inst[k]] = sc[k];
+            }
+        __syncthreads();
+    }
+}
+
+template <typename MT, int W>
+__global__ void __launch_bounds__(512, 1) k_batch_pair(const __grid_constant__ BArgs a, int chunk) {
+    batch_pair_body<MT, W>(a, chunk);
 }
 
 // Order-preserving compaction of the active list (one CTA).
@@ -1031,7 +1381,31 @@ __global__ void k_batch_unscale(BArgs a, int count, const double* __restrict__ x
 // ------------------------------------------------------------------ host side
 struct TuneCfg {
     int threads, chunk, w;  // CTA size, iterations per chunk launch, SELL entries per lane load (1 or 2)
+    int ni;                 // instances per CTA: 1, or 2 (paired form, batches of one shared matrix)
 };
+
+// Candidate shapes of the autotuner: CTA sizes, SELL entry orders and instances per CTA
+// (2 only when every instance shares one matrix).  B2P_BATCH_SHAPE="threads,w,ni" pins
+// all three (the chunk length is still tuned); a pinned pair on a batch of several
+// matrices falls back to one instance per CTA.
+struct ShapeChoices {
+    std::vector<int> threads{128, 256, 512}, w{1, 2}, ni{1, 2};
+};
+
+ShapeChoices shape_choices(BatchWork* w) {
+    ShapeChoices c;
+    const bool can_pair = w->nmat == 1 && w->count > 1;
+    if (!can_pair) c.ni = {1};
+    const char* e = std::getenv("B2P_BATCH_SHAPE");
+    int th = 0, ww = 0, ni = 0;
+    if (e && std::sscanf(e, "%d,%d,%d", &th, &ww, &ni) == 3 && (th == 128 || th == 256 || th == 512) &&
+        (ww == 1 || ww == 2) && (ni == 1 || ni == 2)) {
+        c.threads = {th};
+        c.w = {ww};
+        c.ni = {can_pair ? ni : 1};
+    }
+    return c;
+}
 
 std::string cache_path() {
     const char* p = std::getenv("B2P_AUTOTUNE_CACHE");
@@ -1045,7 +1419,8 @@ std::string batch_key(BatchWork* w, int precision) {
     double mean_m = (double)w->inst_m / w->count, mean_n = (double)w->inst_n / w->count;
     double nnz_col = (double)w->nnz / std::max<int64_t>(w->tot_n, 1);
     std::ostringstream os;
-    os << "batch5_p" << precision << "_c" << (int)std::log2(std::max(1, w->count)) << "_m"
+    const char* f = std::getenv("B2P_BATCH_SHAPE");
+    os << "batch6" << (f && *f ? std::string("_s") + f : std::string()) << "_p" << precision << "_c" << (int)std::log2(std::max(1, w->count)) << "_m"
        << (int)std::log2(mean_m + 1) << "_n" << (int)std::log2(mean_n + 1) << "_k" << (int)std::lround(nnz_col) << "_M"
        << w->max_m << "_N" << w->max_n << "_shared" << (w->nmat == 1 && w->count > 1);
     return os.str();
@@ -1059,7 +1434,7 @@ bool cache_lookup(const std::string& key, TuneCfg* out) {
         std::string k;
         TuneCfg c;
         if (!(is >> k) || k != key) continue;
-        if (is >> c.threads >> c.chunk >> c.w) {
+        if (is >> c.threads >> c.chunk >> c.w >> c.ni) {
             *out = c;
             return true;
         }
@@ -1075,7 +1450,7 @@ void cache_store(const std::string& key, const TuneCfg& c) {
         if (std::system(cmd.c_str()) != 0) return;
     }
     std::ofstream f(p, std::ios::app);
-    f << key << " " << c.threads << " " << c.chunk << " " << c.w << "\n";
+    f << key << " " << c.threads << " " << c.chunk << " " << c.w << " " << c.ni << "\n";
 }
 
 template <typename MT>
@@ -1147,9 +1522,19 @@ BArgs make_args(BatchWork* w, const b2p_params* p, const int32_t* active) {
     return a;
 }
 
-// dynamic shared memory of one CTA: y and xh (MT) of the largest instance
-size_t smem_bytes(BatchWork* w, size_t mt_size) {
-    return mt_size * ((size_t)((w->max_m + 3) & ~3) + (size_t)w->max_n) + 16;
+// dynamic shared memory of one CTA: y and xh (MT) of the largest instance, or of two
+// instances of the shared matrix in the paired form
+size_t smem_bytes(BatchWork* w, size_t mt_size, int ni = 1) {
+    const size_t tab = sizeof(int2) * slice_tab_len((w->max_m + 31) >> 5, (w->max_n + 31) >> 5);
+    if (ni == 2) return tab + mt_size * 2 * ((size_t)((w->max_m + 3) & ~3) + (size_t)((w->max_n + 3) & ~3)) + 16;
+    return tab + mt_size * ((size_t)((w->max_m + 3) & ~3) + (size_t)w->max_n) + 16;
+}
+
+// The chunk kernel of a tuned shape.
+template <typename MT>
+void (*chunk_kernel(int w, int ni))(const BArgs, int) {
+    if (ni == 2) return w == 2 ? k_batch_pair<MT, 2> : k_batch_pair<MT, 1>;
+    return w == 2 ? k_batch_chunk<MT, 2> : k_batch_chunk<MT, 1>;
 }
 
 template <typename MT>
@@ -1183,15 +1568,16 @@ int refill_ell(Ctx* ctx, BatchWork* w, int W) {
     return B2P_OK;
 }
 
-// Times each block size on a size-stratified sample of the batch (no termination,
-// fixed iteration count, no re-centring), then the chunk length: with the chosen block
-// size, launches of a and 4a iterations give the per-iteration cost p and the fixed
-// cost o of a chunk (launch, loading and storing every instance's state, plus the
+// Times each shape on a size-stratified sample of the batch (no termination, 4a
+// iterations -- long enough that the restart checks weigh as in a real solve -- no
+// re-centring), then the chunk length: with the chosen shape, launches of a and 4a
+// iterations give the per-iteration cost p and the fixed cost o of a chunk (launch, loading and storing every instance's state, plus the
 // compaction that follows); the chunk is the shortest power of two from 256 to 8192
 // whose fixed cost is at most 2 % of its iterations -- shorter chunks drop finished
 // instances sooner, so the tail of an uneven batch is cut finer.  Each block size is
-// tried with both SELL entry orders (one entry or a pair per lane load).  Instance
-// state is re-initialised afterwards by the caller.
+// tried with both SELL entry orders (one entry or a pair per lane load) and, when every
+// instance shares one matrix, in the single and the paired form (two instances per
+// CTA).  Instance state is re-initialised afterwards by the caller.
 template <typename MT>
 int autotune(Ctx* ctx, BatchWork* w, const b2p_params* p, TuneCfg* best) {
     std::string key = batch_key(w, sizeof(MT) == 8 ? 0 : 1);
@@ -1209,15 +1595,17 @@ int autotune(Ctx* ctx, BatchWork* w, const b2p_params* p, TuneCfg* best) {
     tp.eps_infeasible = 0.0;
     const int trial_iters = 128;
     float best_ms = 1e30f;
-    *best = {256, 2048, 1};
-    size_t sm = smem_bytes(w, sizeof(MT));
-    for (auto f : {k_batch_chunk<MT, 1>, k_batch_chunk<MT, 2>})
-        B2P_CUDA(ctx, cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-    // one trial launch of `iters` iterations over the sample with `th` threads and entry order
-    // W (ms; < 0: the block size does not fit)
-    auto trial = [&](int th, int W, int iters, float* ms) -> int {
+    *best = {256, 2048, 1, 1};
+    int max_smem = 0;
+    B2P_CUDA(ctx, cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->device));
+    // one trial launch of `iters` iterations over the sample with `th` threads, entry order W
+    // and ni instances per CTA (ms; < 0: the shape does not fit)
+    auto trial = [&](int th, int W, int ni, int iters, float* ms) -> int {
         *ms = -1.0f;
-        auto fn = W == 2 ? k_batch_chunk<MT, 2> : k_batch_chunk<MT, 1>;
+        auto fn = chunk_kernel<MT>(W, ni);
+        const size_t sm = smem_bytes(w, sizeof(MT), ni);
+        if (sm > (size_t)max_smem) return B2P_OK;
+        B2P_CUDA(ctx, cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
         int st = refill_ell(ctx, w, W);
         if (st) return st;
         st = init_instances<MT>(ctx, w, &tp, nullptr, nullptr, nullptr);
@@ -1228,7 +1616,7 @@ int autotune(Ctx* ctx, BatchWork* w, const b2p_params* p, TuneCfg* best) {
         int per_sm = 0;
         B2P_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, th, sm));
         if (per_sm < 1) return B2P_OK;
-        int grid = std::min(sample, ctx->sm_count * per_sm);
+        int grid = std::min((sample + ni - 1) / ni, ctx->sm_count * per_sm);
         cudaEventRecord(ctx->ev0, s);
         fn<<<grid, th, sm, s>>>(a, iters);
         k_batch_compact<<<1, 1024, 0, s>>>(w->ictrl.p, dids.p, w->active2.p, w->counters.p);
@@ -1239,22 +1627,29 @@ int autotune(Ctx* ctx, BatchWork* w, const b2p_params* p, TuneCfg* best) {
         cudaEventElapsedTime(ms, ctx->ev0, ctx->ev1);
         return B2P_OK;
     };
-    for (int W : {1, 2})
-        for (int th : {128, 256, 512}) {
-            float ms = 0.0f;
-            int st = trial(th, W, trial_iters, &ms);
-            if (st) return st;
-            if (ms >= 0.0f && ms < best_ms) {
-                best_ms = ms;
-                best->threads = th;
-                best->w = W;
+    const ShapeChoices choices = shape_choices(w);
+    for (int ni : choices.ni)
+        for (int W : choices.w)
+            for (int th : choices.threads) {
+                float ms = 0.0f;
+                int st = trial(th, W, ni, 4 * trial_iters, &ms);
+                if (st) return st;
+                if (ms >= 0.0f && ms < best_ms) {
+                    best_ms = ms;
+                    best->threads = th;
+                    best->w = W;
+                    best->ni = ni;
+                }
             }
-        }
-    float t4 = 0.0f;
-    int st = trial(best->threads, best->w, 4 * trial_iters, &t4);
+    if (best_ms >= 1e30f) {
+        ctx->err = "batch: no chunk-kernel shape fits this batch";
+        return B2P_INVALID_ARGUMENT;
+    }
+    float t1 = 0.0f;
+    int st = trial(best->threads, best->w, best->ni, trial_iters, &t1);
     if (st) return st;
-    const double per_iter = std::max(1e-9, (double)(t4 - best_ms) / (3.0 * trial_iters));
-    const double fixed = std::max(0.0, (double)best_ms - trial_iters * per_iter);
+    const double per_iter = std::max(1e-9, (double)(best_ms - t1) / (3.0 * trial_iters));
+    const double fixed = std::max(0.0, (double)t1 - trial_iters * per_iter);
     int chunk = 256;
     while (chunk < 8192 && fixed > 0.02 * chunk * per_iter) chunk *= 2;
     best->chunk = chunk;
@@ -1284,11 +1679,12 @@ int batch_run(Ctx* ctx, BatchWork* w, const b2p_params* p, const double* x0_dev,
         }
     }
     w->recenter = false;  // autotune trials run without re-centring
-    TuneCfg cfg = {256, 2048, 1};
+    TuneCfg cfg = {256, 2048, 1, 1};
     if (w->tuned_threads[prec] > 0) {
         cfg.threads = w->tuned_threads[prec];
         cfg.chunk = w->tuned_chunk[prec];
         cfg.w = w->tuned_w[prec];
+        cfg.ni = w->tuned_ni[prec];
     } else {
         if (subset) {
             ctx->err = "subset solve before a full solve of this precision";
@@ -1299,6 +1695,7 @@ int batch_run(Ctx* ctx, BatchWork* w, const b2p_params* p, const double* x0_dev,
         w->tuned_threads[prec] = cfg.threads;
         w->tuned_chunk[prec] = cfg.chunk;
         w->tuned_w[prec] = cfg.w;
+        w->tuned_ni[prec] = cfg.ni;
     }
     {
         int st = refill_ell(ctx, w, cfg.w);
@@ -1350,16 +1747,17 @@ int batch_run(Ctx* ctx, BatchWork* w, const b2p_params* p, const double* x0_dev,
     B2P_CUDA(ctx, cudaMemcpyAsync(w->active.p, act.data(), sizeof(int32_t) * n_act, cudaMemcpyHostToDevice, s));
     int32_t cnt[2] = {0, n_act};
     B2P_CUDA(ctx, cudaMemcpyAsync(w->counters.p, cnt, sizeof(cnt), cudaMemcpyHostToDevice, s));
-    size_t sm = smem_bytes(w, sizeof(MT));
-    auto fn = cfg.w == 2 ? k_batch_chunk<MT, 2> : k_batch_chunk<MT, 1>;
-    B2P_CUDA(ctx, cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    const size_t sm_main = smem_bytes(w, sizeof(MT), cfg.ni);
+    auto fn = chunk_kernel<MT>(cfg.w, cfg.ni);
+    B2P_CUDA(ctx, cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_main));
     int per_sm = 0;
-    B2P_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, cfg.threads, sm));
+    B2P_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, cfg.threads, sm_main));
     if (per_sm < 1) {
         ctx->err = "batch instance too large for one CTA's shared memory";
         return B2P_INVALID_ARGUMENT;
     }
     const int grid = ctx->sm_count * per_sm;
+    const size_t sm = smem_bytes(w, sizeof(MT));  // the wide (single) form
     BArgs a1 = make_args<MT>(w, p, w->active.p);
     BArgs a2 = make_args<MT>(w, p, w->active2.p);
     // the wide form for the tail: 1024 threads, one CTA per SM
@@ -1390,10 +1788,10 @@ int batch_run(Ctx* ctx, BatchWork* w, const b2p_params* p, const double* x0_dev,
     cudaGraphExec_t& exec_w = own.exec[1];
     for (int g = 0; g < (have_wide ? 2 : 1); ++g) {
         B2P_CUDA(ctx, cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
-        if (g == 0) fn<<<grid, cfg.threads, sm, s>>>(a1, cfg.chunk);
+        if (g == 0) fn<<<grid, cfg.threads, sm_main, s>>>(a1, cfg.chunk);
         else fnw<<<grid_w, 1024, sm, s>>>(a1, cfg.chunk);
         k_batch_compact<<<1, 1024, 0, s>>>(w->ictrl.p, w->active.p, w->active2.p, w->counters.p);
-        if (g == 0) fn<<<grid, cfg.threads, sm, s>>>(a2, cfg.chunk);
+        if (g == 0) fn<<<grid, cfg.threads, sm_main, s>>>(a2, cfg.chunk);
         else fnw<<<grid_w, 1024, sm, s>>>(a2, cfg.chunk);
         k_batch_compact<<<1, 1024, 0, s>>>(w->ictrl.p, w->active2.p, w->active.p, w->counters.p);
         cudaGraph_t& gr = g == 0 ? graph : graph_w;
@@ -1508,7 +1906,7 @@ void fill_summary(b2p_result* sum, int count, bool timed_out, int64_t tot_it, in
     sum->kernel_time_ms = kms;
     sum->primal_weight = 0.0;
     sum->step_size = cfg.threads * 100000.0 + cfg.chunk;  // tuned block size * 1e5 + chunk length
-    sum->used_average = cfg.w;                              // SELL entries per lane load
+    sum->used_average = 10 * cfg.ni + cfg.w;                // 10 * instances per CTA + SELL entries per lane load
 }
 
 // All instances of the batch share one shape (required by the learned warm start).
@@ -1643,6 +2041,10 @@ int b2p_batch_upload(void* p, int nmat, const int32_t* mat_m, const int32_t* mat
             c_pad += 32LL * ((clen[cord[s0]] + 1) & ~1);
         }
         c_sptr.push_back(c_pad);
+        if (r_pad > INT32_MAX || c_pad > INT32_MAX) {  // the kernels' slice tables hold 32-bit offsets
+            ctx->err = "b2p_batch_upload: the batch's padded matrices exceed 2^31 entries; split the batch";
+            return B2P_INVALID_ARGUMENT;
+        }
         rp_base += m + 1;
     }
     w->h_mat_m.assign(mat_m, mat_m + nmat);

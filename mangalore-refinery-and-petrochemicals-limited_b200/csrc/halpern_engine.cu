@@ -608,33 +608,40 @@ __global__ void __launch_bounds__(1024) k_iter_sell(IterArgs<VT, GT> a, int it) 
         const int* ip = a.idx + p0 + rl * W;
         VT s_0 = (VT)0, s_1 = (VT)0;
         // chunk q of this row at vp + q C W; lane group `sub` takes q = sub, sub + LPR, ...
-        int q = sub;
-        for (; q + LPR < nq; q += 2 * LPR) {
-            VT v0[W], v1[W];
-            int c0[W], c1[W];
-            ld_stream_w<W>(vp + (int64_t)q * C * W, v0, pol);
-            ld_stream_w<W>(ip + (int64_t)q * C * W, c0, pol);
-            ld_stream_w<W>(vp + (int64_t)(q + LPR) * C * W, v1, pol);
-            ld_stream_w<W>(ip + (int64_t)(q + LPR) * C * W, c1, pol);
-            GT g0[W], g1[W];
+        // U chunks (8 entries per lane) per step: every value and index load of the step
+        // (the last step predicated on the row's length) is issued before the first
+        // gather, and every gather before the first multiply, so a step costs two
+        // dependent L2 round trips for 8 entries
+        constexpr int U = W >= 8 ? 1 : 8 / W;
+        for (int q = sub; q < nq; q += U * LPR) {
+            VT v[U][W];
+            int c[U][W];
 #pragma unroll
-            for (int e = 0; e < W; ++e) {
-                g0[e] = gat(c0[e]);
-                g1[e] = gat(c1[e]);
+            for (int u = 0; u < U; ++u) {
+                const int qq = q + u * LPR;
+                if (qq < nq) {
+                    ld_stream_w<W>(vp + (int64_t)qq * C * W, v[u], pol);
+                    ld_stream_w<W>(ip + (int64_t)qq * C * W, c[u], pol);
+                } else {
+#pragma unroll
+                    for (int e = 0; e < W; ++e) {
+                        v[u][e] = (VT)0;
+                        c[u][e] = -1;
+                    }
+                }
             }
+            GT g[U][W];
 #pragma unroll
-            for (int e = 0; e < W; ++e) {
-                s_0 += v0[e] * (VT)g0[e];
-                s_1 += v1[e] * (VT)g1[e];
-            }
-        }
-        if (q < nq) {
-            VT v0[W];
-            int c0[W];
-            ld_stream_w<W>(vp + (int64_t)q * C * W, v0, pol);
-            ld_stream_w<W>(ip + (int64_t)q * C * W, c0, pol);
+            for (int u = 0; u < U; ++u)
 #pragma unroll
-            for (int e = 0; e < W; ++e) s_0 += v0[e] * (VT)gat(c0[e]);
+                for (int e = 0; e < W; ++e) g[u][e] = c[u][e] >= 0 ? gat(c[u][e]) : (GT)0;
+#pragma unroll
+            for (int u = 0; u < U; ++u)
+#pragma unroll
+                for (int e = 0; e < W; ++e) {
+                    if (u & 1) s_1 += v[u][e] * (VT)g[u][e];
+                    else s_0 += v[u][e] * (VT)g[u][e];
+                }
         }
         VT s = s_0 + s_1;
 #pragma unroll
@@ -822,7 +829,7 @@ __global__ void __launch_bounds__(TB) k_kkt_rows(int m, const int32_t* __restric
     const int lane = threadIdx.x & 31, sub = lane & (L - 1), rpw = 32 / L;
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
     const bool rays = xd != nullptr;
-    double p2 = 0.0, by = 0.0, est = 0.0, prv = 0.0, drb = 0.0, drm = 0.0;
+    double p2 = 0.0, by = 0.0, est = 0.0, prv = 0.0, drb = 0.0, drm = 0.0, ysv = 0.0;
     for (int base = warp * rpw; base < m; base += nw * rpw) {
         int r = base + lane / L;
         bool valid = r < m;
@@ -846,6 +853,7 @@ __global__ void __launch_bounds__(TB) k_kkt_rows(int m, const int32_t* __restric
             const double yv = (map.ybar ? map.ybar[r] : 0.0) + ds * (dr[r] * (double)yt[r]);
             by += b[r] * yv;
             est += fabs(yv) * fabs(rp);
+            if (!eq && yv < 0.0) ysv += yv * yv;  // y >= 0 on <= rows: part of the dual residual
             if (rays) {
                 const double adx = sd / dr[r];  // (A dx)_r, original space
                 const double v = eq ? adx : fmax(adx, 0.0);
@@ -859,6 +867,7 @@ __global__ void __launch_bounds__(TB) k_kkt_rows(int m, const int32_t* __restric
     block_sum_to(p2, &ctrl->acc[A_PRES2]);
     block_sum_to(by, &ctrl->acc[A_BY]);
     block_sum_to(est, &ctrl->acc[A_EST]);
+    block_sum_to(ysv, &ctrl->acc[A_DRES2]);
     if (rays) {
         block_sum_to(prv, &ctrl->acc[A_PRV2]);
         block_sum_to(drb, &ctrl->acc[A_DRB]);

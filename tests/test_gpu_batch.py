@@ -241,3 +241,44 @@ def test_batch_trace_and_objectives(ctx, lpgen):
         assert abs(obj["pobj"][i] - k["pobj"]) <= 1e-9 * max(1.0, abs(k["pobj"]))
         assert abs(obj["dobj"][i] - k["dobj"]) <= 1e-6 * max(1.0, abs(k["dobj"]))
         assert np.isfinite(obj["obj_err"][i]) and obj["obj_err"][i] >= 0.0
+
+
+@pytest.mark.parametrize("precision", ["fp32", "fp64"])
+def test_batch_pair_form_matches_single(b2p, lpgen, tmp_path, monkeypatch, precision):
+    """The paired form (two instances of the shared matrix per CTA, each SELL load
+    feeding both instances' gathers) reproduces the single form bit for bit at the
+    same CTA size and entry order: statuses, iteration counts and answers.  63
+    planning instances, so one CTA holds an unpaired instance, and pairs part when one
+    member finishes first."""
+    monkeypatch.setenv("B2P_AUTOTUNE_CACHE", str(tmp_path / "tune.txt"))
+    fam = lpgen.RefineryPlanningFamily()
+    P = fam.sample_params(63, 777)
+    out = {}
+    for ni in (1, 2):
+        monkeypatch.setenv("B2P_BATCH_SHAPE", f"256,2,{ni}")
+        c = b2p.Context(0)
+        try:
+            b2p.warmstart.upload_family(c, fam, P)
+            summ, per, x, y = c.batch_solve(precision=precision, eps=1e-5, max_iterations=30000)
+            assert int(round(summ["used_average"])) == 10 * ni + 2
+            assert int(round(summ["step_size"])) // 100000 == 256
+            out[ni] = (per, x, y)
+        finally:
+            c.close()
+    (p1, x1, y1), (p2, x2, y2) = out[1], out[2]
+    assert np.array_equal(p1["status"], p2["status"])
+    assert np.array_equal(p1["iterations"], p2["iterations"])
+    assert len(set(p1["iterations"].tolist())) > 1  # instances finish at different iterations
+    assert np.array_equal(x1, x2) and np.array_equal(y1, y2)
+
+
+def test_batch_pair_form_chosen_only_for_shared_matrix(ctx, lpgen, tmp_path, monkeypatch):
+    """A pinned paired shape on a batch of different matrices runs one instance per CTA."""
+    monkeypatch.setenv("B2P_AUTOTUNE_CACHE", str(tmp_path / "tune.txt"))
+    monkeypatch.setenv("B2P_BATCH_SHAPE", "256,1,2")
+    stds = upload_lps(ctx, lpgen.uneven_batch(12, m_hi=300, seed=46))
+    summ, per, x, y = ctx.batch_solve(precision="fp32", eps=1e-6, max_iterations=100000)
+    assert int(round(summ["used_average"])) == 11
+    assert np.all(per["status"] == 0)
+    for s, (xi, yi) in zip(stds, split(stds, x, y)):
+        assert pdlp_oracle.kkt(s, xi, yi)["rel_kkt"] <= 1.05e-6
