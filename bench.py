@@ -41,7 +41,7 @@ sys.path.insert(0, str(ROOT))
 # extrapolates the reference CPU solver's per-iteration cost over this many
 # iterations -- generous to the CPU: the reference's own vanilla PDHG needs far
 # more iterations and never reaches 1e-6 on these LPs.
-HALPERN_ITERS = {"block_angular": 6784, "random_sparse": 5056, "refinery_learned": 65388, "uneven_batch": 6207,
+HALPERN_ITERS = {"block_angular": 6784, "random_sparse": 5056, "refinery_learned": 114034, "uneven_batch": 6379,
                  # mixed engine to 1e-8 (the FP64 leg of this workload was not run)
                  "ill_conditioned": 1230784}
 
@@ -671,6 +671,7 @@ def run_learned_workload(args):
             launches = int(summ["kernel_launches"]) * k
             it_total = float(per["iterations"].sum())
             kern_ms = summ["kernel_time_ms"]
+            ni = max(1, int(round(summ["used_average"])) // 10)  # instances per CTA of the tuned shape
     # end to end through the public API: pinned host parameter vectors and instance
     # data -> upload -> learned solve -> answers to host
     _, B, Cc, LB, UB, EQ = fam.standard_batch(P)
@@ -693,16 +694,19 @@ def run_learned_workload(args):
                "d2h_bytes_per_step": d2h, "steps": args.e2e_steps, "ms_per_step": e2e_ms / args.e2e_steps,
                "solved": int(esolved),
                "note": "batch upload (host CSR checks, renumbering, device transpose, scaling) + learned solve + x, y"}
-    # roofline of the dominant kernel (k_batch_chunk<float>): algorithmic bytes of every
-    # instance-iteration of the value leg over its kernel time.  The shared matrix and the
-    # instances' vectors are served from L2 and shared memory, so the bound that applies is
-    # the on-chip one; the DRAM share comes from the committed ncu capture.
+    # roofline of the dominant kernel (the batched chunk kernel of the tuned shape):
+    # algorithmic bytes of every instance-iteration of the value leg over its kernel time --
+    # the SELL matrix (12 B per nonzero, both orientations) once per CTA-iteration, so once
+    # per ni instances, plus each instance's vectors.  The shared matrix and the vectors are
+    # served from L2 and shared memory, so the bound that applies is the on-chip one; the
+    # DRAM share comes from the committed ncu capture.
     nnz = int(fam.rowptr[-1])
-    per_iter = 12 * nnz + 24 * fam.n + 16 * fam.m
+    per_iter = 12 * nnz / ni + 24 * fam.n + 16 * fam.m
     pk, pk_src = peaks()
     peak = pk["hbm_gbs"]
     achieved = it_total * per_iter / (kern_ms / 1e3) / 1e9
-    prof = read_profile(ROOT / "profiles" / "batch_chunk_refinery_planning.txt")
+    kname = "k_batch_pair" if ni == 2 else "k_batch_chunk"
+    prof = read_profile(ROOT / "profiles" / f"{kname[2:]}_refinery_planning.txt")
     roofline = {"bound": "l2", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "traffic": prof.get("dram_bytes_per_instance_iteration"),
                 "traffic_unit": "DRAM bytes per instance-iteration (ncu dram__bytes_read.sum + write.sum)",
@@ -710,12 +714,13 @@ def run_learned_workload(args):
                               if "dram_bytes_per_instance_iteration" in prof else None),
                 "l2_bytes_per_instance_iteration": prof.get("l2_bytes_per_instance_iteration"),
                 "lts_throughput_pct": prof.get("lts_throughput_pct"),
-                "kernel": "k_batch_chunk<float> (SELL, learned leg)",
+                "kernel": f"{kname}<float> (SELL, {ni} instance(s) per CTA, learned leg)",
                 "algorithmic_bytes_per_instance_iteration": per_iter,
                 "peak_source": "hbm_gbs: " + pk_src + "; no measured L2 peak exists, so the fraction is against HBM",
-                "note": "12 B per nonzero (FP32 value + 16-bit index, both orientations), 24 B per column, 16 B per "
-                        "row; bound 'l2': the shared matrix and the instances' vectors stay in L2 / shared memory "
-                        "(ncu: DRAM carries dram_frac of these bytes)"}
+                "note": f"12 B per nonzero (FP32 value + 16-bit index, both orientations) shared by the {ni} "
+                        "instance(s) of a CTA, 24 B per column, 16 B per row; bound 'l2': the shared matrix and "
+                        "the instances' vectors stay in L2 / shared memory (ncu: DRAM carries dram_frac of these "
+                        "bytes)"}
     # training on the tensor cores: GEMM FLOPs of all epochs (per sample: layer 1 forward +
     # weight gradient, layers 2 and 3 forward + weight gradient + input gradient) over the
     # training time, against the sustained BF16 peak
@@ -821,10 +826,14 @@ def run_reference_learned(args):
             vals.append(len(out) / max(per_lp))
     wall = time.perf_counter() - t0
     v = statistics.median(vals)
-    cb = {"value": v, "unit": "LPs/s", "cores": cores, "kind": "reference",
+    cb = {"value": v, "unit": "LPs/s", "cores": cores, "kind": "reference", "extrapolated": True,
           "sample": (f"reference CPUFirstOrderSolver (compiled from its sources), {cores} processes x 1 held-out "
                      f"instance each: runs of 1 and {1 + _ref_worker.sample} iterations; per-LP time = setup + "
-                     f"{iters} x per-iteration (the FP64 engine's mean iteration count to 1e-6); {wall:.1f} s wall")}
+                     f"{iters} x per-iteration; {wall:.1f} s wall"),
+          "extrapolation": (f"the reference's plain PDHG does not reach 1e-6 relative KKT on these LPs (it stops at "
+                            f"its iteration limit); its measured per-iteration cost is multiplied by {iters}, the "
+                            f"mean iteration count of the B200 FP64 Halpern engine (a different, restarted "
+                            f"algorithm) on the 2,000 held-out instances -- generous to the CPU")}
     line = {"metric": METRIC_LEARNED, "value": v, "unit": "LPs/s", "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1e3 / v, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded refinery planning family, no dataset)",

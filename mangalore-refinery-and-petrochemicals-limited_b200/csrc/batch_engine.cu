@@ -134,7 +134,6 @@ void batch_free(Ctx* ctx) {
 namespace {
 
 constexpr int kLongSlice = 128;  // entries per lane above which a slice is summed warp-cooperatively
-constexpr int kKktLanesCol = 4, kKktLanesRow = 8;
 
 // Packed per-column / per-row parameters of the scaled (and, when re-centred,
 // shifted) problem in the solve's precision.
@@ -158,6 +157,7 @@ struct BArgs {
     const int64_t *r_sptr, *c_sptr, *mat_rs_off, *mat_cs_off;
     const uint16_t *r_eidx, *c_eidx;
     const void *r_ev, *c_ev;  // MT-typed
+    const double *r_ev64, *c_ev64;  // FP64 values in the same order (restart-check KKT)
     const int32_t *r_ext, *c_ext;
     // instances
     const int32_t* inst_mat;
@@ -216,47 +216,53 @@ __device__ __forceinline__ void block_sums(double (&v)[NV], double* sh /* [32*NV
 // value and index load of a batch (the last batch predicated on the row's length)
 // is issued before the first gather that needs one, so a slice of up to B entries
 // per lane costs one L2 round trip and a longer one a round trip per batch.
-template <typename MT, int W>
-__device__ __forceinline__ MT ell_dot(const MT* __restrict__ v, const uint16_t* __restrict__ ix, int len,
-                                      const MT* __restrict__ g) {
-    constexpr int B = sizeof(MT) == 4 ? 8 : 4;
-    MT s = (MT)0;
+template <typename VT, typename GT, int W>
+__device__ __forceinline__ VT ell_dot_vg(const VT* __restrict__ v, const uint16_t* __restrict__ ix, int len,
+                                        const GT* __restrict__ g) {
+    constexpr int B = sizeof(VT) == 4 ? 8 : 4;
+    VT s = (VT)0;
     if constexpr (W == 1) {
         for (int q = 0; q < len; q += B) {
-            MT vv[B];
+            VT vv[B];
             unsigned ii[B];
 #pragma unroll
             for (int u = 0; u < B; ++u) {
                 const bool h = q + u < len;
-                vv[u] = h ? v[(q + u) * 32] : (MT)0;
+                vv[u] = h ? v[(q + u) * 32] : (VT)0;
                 ii[u] = h ? (unsigned)ix[(q + u) * 32] : 0u;
             }
 #pragma unroll
             for (int u = 0; u < B; ++u)
-                if (q + u < len) s += vv[u] * g[ii[u]];
+                if (q + u < len) s += vv[u] * (VT)g[ii[u]];
         }
     } else {
-        typedef typename std::conditional<sizeof(MT) == 4, float2, double2>::type MT2;
+        typedef typename std::conditional<sizeof(VT) == 4, float2, double2>::type VT2;
         constexpr int P = B / 2;  // pairs per batch
         const int np = len >> 1;
         for (int t = 0; t < np; t += P) {
-            MT2 vv[P];
+            VT2 vv[P];
             unsigned ii[P];
 #pragma unroll
             for (int u = 0; u < P; ++u) {
                 const bool h = t + u < np;
-                vv[u] = h ? *reinterpret_cast<const MT2*>(v + (t + u) * 64) : MT2{(MT)0, (MT)0};
+                vv[u] = h ? *reinterpret_cast<const VT2*>(v + (t + u) * 64) : VT2{(VT)0, (VT)0};
                 ii[u] = h ? *reinterpret_cast<const unsigned*>(ix + (t + u) * 64) : 0u;
             }
 #pragma unroll
             for (int u = 0; u < P; ++u)
                 if (t + u < np) {
-                    s += vv[u].x * g[ii[u] & 0xFFFFu];
-                    s += vv[u].y * g[ii[u] >> 16];
+                    s += vv[u].x * (VT)g[ii[u] & 0xFFFFu];
+                    s += vv[u].y * (VT)g[ii[u] >> 16];
                 }
         }
     }
     return s;
+}
+
+template <typename MT, int W>
+__device__ __forceinline__ MT ell_dot(const MT* __restrict__ v, const uint16_t* __restrict__ ix, int len,
+                                      const MT* __restrict__ g) {
+    return ell_dot_vg<MT, MT, W>(v, ix, len, g);
 }
 
 // ell_dot for two instances of one matrix: every value and index load of the slice
@@ -336,14 +342,14 @@ __device__ __forceinline__ int snake_slice(int r, int w, int nw) { return r * nw
 // The 32 rows of one slice summed by the whole warp over the CSR copy (rows
 // first .. first+cnt-1, global numbering; `off` localises the column index).
 // Lane r returns the sum of row first + r.
-template <typename MT>
+template <typename MT, typename GT = MT>
 __device__ MT long_slice_dot(const MT* __restrict__ vals, const int32_t* __restrict__ ptr,
                              const int32_t* __restrict__ idx, int64_t first, int cnt, int64_t off,
-                             const MT* __restrict__ g, int lane) {
+                             const GT* __restrict__ g, int lane) {
     MT mine = (MT)0;
     for (int r = 0; r < cnt; ++r) {
         MT s = (MT)0;
-        for (int e = ptr[first + r] + lane; e < ptr[first + r + 1]; e += 32) s += vals[e] * g[idx[e] - off];
+        for (int e = ptr[first + r] + lane; e < ptr[first + r + 1]; e += 32) s += vals[e] * (MT)g[idx[e] - off];
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
         if (lane == r) mine = s;
@@ -430,36 +436,46 @@ __device__ __forceinline__ void restart_instance(const BArgs& a, int m, int n, i
 // global memory: the FP64 KKT of T(z) on the original instance, the objective-error
 // bound, the certificates (every fourth check) and the decisions -- termination,
 // restart, primal weight -- which thread 0 writes to `sc` and `s_flags` (0: done,
-// 1: restart).  Kept out of line: its FP64 accumulators would otherwise raise the
-// register demand of the iteration loop.
-template <typename MT>
+// 1: restart).  The products A xt, A^T yt (and A dx, A^T dy) run over the FP64 SELL
+// copies of the scaled matrix with the slice table `tab`, one lane per row / column as
+// in the iterations, gathering from `buf` -- the instance's xh region of shared memory,
+// free at a check (the dual phase has consumed xh, the next primal phase rewrites it) --
+// into which each gathered vector is staged first.  Kept out of line: its FP64
+// accumulators would otherwise raise the register demand of the iteration loop.
+template <typename MT, int W>
 __device__ __noinline__ void check_instance(const BArgs& a, int inst, int m, int n, int64_t ro, int64_t co,
                                             int64_t xo, int64_t yo, long long total, long long kk, double om,
                                             double r_now, double dxa, double dya, InstCtrl& sc, int* s_flags,
-                                            double* red) {
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
-    const int csub = lane & (kKktLanesCol - 1), cgid = warp * (32 / kKktLanesCol) + lane / kKktLanesCol;
-    const int cgroups = nwarps * (32 / kKktLanesCol);
-    const int rsub = lane & (kKktLanesRow - 1), rgid = warp * (32 / kKktLanesRow) + lane / kKktLanesRow;
-    const int rgroups = nwarps * (32 / kKktLanesRow);
+                                            double* red, const int2* tab, MT* buf) {
+    const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5, nwarps = nt >> 5;
+    const int ncs = (n + 31) >> 5, nrs = (m + 31) >> 5;
     const MT *xtg = (const MT*)a.xt, *ytg = (const MT*)a.yt;
     const MT *dxg = (const MT*)a.dx, *dyg = (const MT*)a.dy;
     const bool rays = a.eps_inf > 0.0;
-    // ---- FP64 KKT of T(z) on the original instance (CSR, sub-warp per row / column) and the
-    // objective-error bound
+    // (A v)_i in the scaled space for lane `lane` of row slice sl, v staged in buf
+    auto row_dot = [&](int sl) -> double {
+        const int2 t = tab[ncs + sl];
+        return t.y <= kLongSlice
+                   ? ell_dot_vg<double, MT, W>(a.r_ev64 + t.x + W * lane, a.r_eidx + t.x + W * lane, t.y, buf)
+                   : long_slice_dot<double, MT>(a.sv64, a.rowptr, a.colidx, ro + (sl << 5), min(32, m - (sl << 5)),
+                                                co, buf, lane);
+    };
+    auto col_dot = [&](int sl) -> double {
+        const int2 t = tab[sl];
+        return t.y <= kLongSlice
+                   ? ell_dot_vg<double, MT, W>(a.c_ev64 + t.x + W * lane, a.c_eidx + t.x + W * lane, t.y, buf)
+                   : long_slice_dot<double, MT>(a.stv64, a.t_rowptr, a.t_colidx, co + (sl << 5),
+                                                min(32, n - (sl << 5)), ro, buf, lane);
+    };
+    // ---- FP64 KKT of T(z) on the original instance and the objective-error bound
     double kk2[6] = {0, 0, 0, 0, 0, 0};
     // |primal residual|^2, b.y, |dual residual|^2, c.x, bound term, sum |y| viol
-    for (int base = 0; base < m; base += rgroups) {
-        const int i = base + rgid;
-        double s = 0.0;
+    for (int j = tid; j < n; j += nt) buf[j] = xtg[xo + j];
+    __syncthreads();
+    for (int sl = warp; sl < nrs; sl += nwarps) {
+        const int i = (sl << 5) + lane;
+        const double s = row_dot(sl);
         if (i < m) {
-            const int64_t gi = ro + i;
-            for (int e = a.rowptr[gi] + rsub; e < a.rowptr[gi + 1]; e += kKktLanesRow)
-                s += a.sv64[e] * (double)xtg[xo + a.colidx[e] - co];
-        }
-#pragma unroll
-        for (int o = kKktLanesRow / 2; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-        if (i < m && rsub == 0) {
             const double dri = a.dr[ro + i];
             const double ax = (a.recenter ? a.axbar[yo + i] : 0.0) + s / dri;
             double rp = ax - a.b[yo + i];
@@ -471,17 +487,13 @@ __device__ __noinline__ void check_instance(const BArgs& a, int inst, int m, int
             if (!a.is_eq[yo + i] && yv < 0.0) kk2[2] += yv * yv;  // y >= 0 on <= rows (dual residual)
         }
     }
-    for (int base = 0; base < n; base += cgroups) {
-        const int j = base + cgid;
-        double s = 0.0;
+    __syncthreads();  // every warp is done with xt
+    for (int i = tid; i < m; i += nt) buf[i] = ytg[yo + i];
+    __syncthreads();
+    for (int sl = warp; sl < ncs; sl += nwarps) {
+        const int j = (sl << 5) + lane;
+        const double s = col_dot(sl);
         if (j < n) {
-            const int64_t gj = co + j;
-            for (int e = a.t_rowptr[gj] + csub; e < a.t_rowptr[gj + 1]; e += kKktLanesCol)
-                s += a.stv64[e] * (double)ytg[yo + a.t_colidx[e] - ro];
-        }
-#pragma unroll
-        for (int o = kKktLanesCol / 2; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-        if (j < n && csub == 0) {
             const double dcj = a.dc[co + j];
             const double cj = a.c[xo + j], lj = a.lb[xo + j], uj = a.ub[xo + j];
             const double g = cj + (a.recenter ? a.atybar[xo + j] : 0.0) + s / dcj;
@@ -501,17 +513,12 @@ __device__ __noinline__ void check_instance(const BArgs& a, int inst, int m, int
     double ry[7] = {0, 0, 0, 0, 0, 0, 0};
     const bool ray_check = rays && ((total / a.K) & 3) == 0;
     if (ray_check) {
-        for (int base = 0; base < m; base += rgroups) {
-            const int i = base + rgid;
-            double s = 0.0;
+        for (int j = tid; j < n; j += nt) buf[j] = dxg[xo + j];
+        __syncthreads();
+        for (int sl = warp; sl < nrs; sl += nwarps) {
+            const int i = (sl << 5) + lane;
+            const double s = row_dot(sl);
             if (i < m) {
-                const int64_t gi = ro + i;
-                for (int e = a.rowptr[gi] + rsub; e < a.rowptr[gi + 1]; e += kKktLanesRow)
-                    s += a.sv64[e] * (double)dxg[xo + a.colidx[e] - co];
-            }
-#pragma unroll
-            for (int o = kKktLanesRow / 2; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-            if (i < m && rsub == 0) {
                 const double dri = a.dr[ro + i];
                 const double adx = s / dri;  // (A dx)_i in the original space
                 const double v = a.is_eq[yo + i] ? adx : fmax(adx, 0.0);
@@ -521,17 +528,13 @@ __device__ __noinline__ void check_instance(const BArgs& a, int inst, int m, int
                 ry[5] += fabs(a.b[yo + i] * dyo);
             }
         }
-        for (int base = 0; base < n; base += cgroups) {
-            const int j = base + cgid;
-            double s = 0.0;
+        __syncthreads();
+        for (int i = tid; i < m; i += nt) buf[i] = dyg[yo + i];
+        __syncthreads();
+        for (int sl = warp; sl < ncs; sl += nwarps) {
+            const int j = (sl << 5) + lane;
+            const double s = col_dot(sl);
             if (j < n) {
-                const int64_t gj = co + j;
-                for (int e = a.t_rowptr[gj] + csub; e < a.t_rowptr[gj + 1]; e += kKktLanesCol)
-                    s += a.stv64[e] * (double)dyg[yo + a.t_colidx[e] - ro];
-            }
-#pragma unroll
-            for (int o = kKktLanesCol / 2; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-            if (j < n && csub == 0) {
                 const double dcj = a.dc[co + j];
                 const double cj = a.c[xo + j], lj = a.lb[xo + j], uj = a.ub[xo + j];
                 const bool fl = isfinite(lj), fu = isfinite(uj);
@@ -752,7 +755,8 @@ __device__ __forceinline__ void batch_chunk_body(const BArgs& a, int chunk) {
                 dya = sqrt(acc[3]);
             }
             __syncthreads();  // xt / yt of this iteration are in global memory
-            check_instance<MT>(a, inst, m, n, ro, co, xo, yo, total, kk, om, r_now, dxa, dya, sc, s_flags, red);
+            check_instance<MT, W>(a, inst, m, n, ro, co, xo, yo, total, kk, om, r_now, dxa, dya, sc, s_flags, red,
+                                  tab, xhs);
             __syncthreads();
             done = s_flags[0] != 0;
             om = sc.omega;
@@ -822,7 +826,7 @@ __device__ __forceinline__ void batch_pair_body(const BArgs& a, int chunk) {
     const int64_t* csp = a.c_sptr + a.mat_cs_off[0];
     const int nrs = (m + 31) >> 5, ncs = (n + 31) >> 5;
     const double eta = a.mat_eta[0];
-    const int m4 = (m + 3) & ~3, stride = m4 + ((n + 3) & ~3);
+    const int m4 = (m + 3) & ~3, stride = m4 + max((n + 3) & ~3, m4);  // xh region also stages y at checks
     int2* tab = (int2*)smem_raw;  // column slices, then row slices (built once: one matrix)
     MT* ysb[2] = {(MT*)(tab + slice_tab_len(nrs, ncs)), (MT*)(tab + slice_tab_len(nrs, ncs)) + stride};
     MT* xhb[2] = {ysb[0] + m4, ysb[1] + m4};
@@ -1013,8 +1017,8 @@ __device__ __forceinline__ void batch_pair_body(const BArgs& a, int chunk) {
                     dya = sqrt(acc[k][3]);
                 }
                 __syncthreads();
-                check_instance<MT>(a, inst[k], m, n, ro, co, xo[k], yo[k], total[k], kk[k], om[k], r_now, dxa, dya,
-                                   sc[k], s_flags[k], red);
+                check_instance<MT, W>(a, inst[k], m, n, ro, co, xo[k], yo[k], total[k], kk[k], om[k], r_now, dxa,
+                                      dya, sc[k], s_flags[k], red, tab, xhb[k]);
                 __syncthreads();
                 live[k] = s_flags[k][0] == 0;
                 om[k] = sc[k].omega;
@@ -1171,7 +1175,6 @@ __global__ void k_batch_power(int nmat, const int32_t* __restrict__ mat_m, const
             s_stop = 0;
         }
         __syncthreads();
-        double est = 0.0;
         for (int t = 0; t < 1000 && !s_stop; ++t) {
             const double inv = 1.0 / s_norm;
             for (int i = threadIdx.x; i < m; i += blockDim.x) {
@@ -1191,7 +1194,6 @@ __global__ void k_batch_power(int nmat, const int32_t* __restrict__ mat_m, const
             block_sums<1>(w, red);
             if (threadIdx.x == 0) {
                 double nn = sqrt(w[0]);
-                est = nn;
                 if (nn <= 0.0 || fabs(nn - s_prev) <= 1e-7 * nn) s_stop = 1;
                 s_prev = nn;
                 s_norm = nn > 0.0 ? nn : 1.0;
@@ -1480,6 +1482,8 @@ BArgs make_args(BatchWork* w, const b2p_params* p, const int32_t* active) {
     a.c_eidx = w->c_eidx.p;
     a.r_ev = f64 ? (const void*)w->r_ev64.p : (const void*)w->r_ev32.p;
     a.c_ev = f64 ? (const void*)w->c_ev64.p : (const void*)w->c_ev32.p;
+    a.r_ev64 = w->r_ev64.p;
+    a.c_ev64 = w->c_ev64.p;
     a.r_ext = w->r_ext.p;
     a.c_ext = w->c_ext.p;
     a.inst_mat = w->inst_mat.p;
@@ -1526,8 +1530,8 @@ BArgs make_args(BatchWork* w, const b2p_params* p, const int32_t* active) {
 // instances of the shared matrix in the paired form
 size_t smem_bytes(BatchWork* w, size_t mt_size, int ni = 1) {
     const size_t tab = sizeof(int2) * slice_tab_len((w->max_m + 31) >> 5, (w->max_n + 31) >> 5);
-    if (ni == 2) return tab + mt_size * 2 * ((size_t)((w->max_m + 3) & ~3) + (size_t)((w->max_n + 3) & ~3)) + 16;
-    return tab + mt_size * ((size_t)((w->max_m + 3) & ~3) + (size_t)w->max_n) + 16;
+    const size_t m4 = (size_t)((w->max_m + 3) & ~3), n4 = (size_t)((w->max_n + 3) & ~3);
+    return tab + mt_size * ni * (m4 + std::max(n4, m4)) + 16;  // y, then xh (which also stages y at checks)
 }
 
 // The chunk kernel of a tuned shape.
