@@ -399,6 +399,12 @@ __device__ __forceinline__ void ld_stream_w(const int* p, int (&v)[W], unsigned 
     }
 }
 
+// Bulk prefetch of a byte range into L2 (no registers, no completion to wait for); the
+// range must start on a 16-byte boundary and its size be a multiple of 16 bytes.
+__device__ __forceinline__ void prefetch_l2(const void* p, unsigned bytes) {
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
+}
+
 // L lanes per row, R rows per lane group per step.  Within a step every load that
 // does not depend on another -- the R row-pointer pairs, the R epilogue operands,
 // the first L entries of the R rows, then their R gathers -- is issued before any
@@ -593,6 +599,17 @@ __global__ void __launch_bounds__(1024) k_iter_sell(IterArgs<VT, GT> a, int it) 
         const bool lead = valid && sub == 0;
         const long long p0 = ld_stream((const long long*)a.soff + sl, pol);
         const long long p1 = ld_stream((const long long*)a.soff + sl + 1, pol);
+        // the warp's next slice goes to L2 while this one is summed: its value and index
+        // loads then wait on L2, not on DRAM (slice offsets are multiples of C W entries,
+        // so both ranges start and end on 16-byte boundaries)
+        if (lane == 0 && sl + wpc < s1) {
+            const long long q0 = ld_stream((const long long*)a.soff + sl + wpc, pol);
+            const long long q1 = ld_stream((const long long*)a.soff + sl + wpc + 1, pol);
+            if (q1 > q0) {
+                prefetch_l2(a.val + q0, (unsigned)((q1 - q0) * sizeof(VT)));
+                prefetch_l2(a.idx + q0, (unsigned)((q1 - q0) * sizeof(int)));
+            }
+        }
         const VT zr = lead ? a.z[row] : (VT)0;
         const VT cst = lead ? a.cost[row] : (VT)0;
         const VT zan = lead ? a.za[row] : (VT)0;
