@@ -63,8 +63,9 @@ def peaks():
 # Seconds of each part of the refinery_learned run on one B200 (2,000 held-out
 # instances; labels to 1e-8, legs to 1e-6 relative KKT with the answer's objective
 # within 1e-6), used to plan the run's wall time from its leg counts.
-LEARNED_LEG_S = {"start": 20.0, "label_per_instance": 0.0156, "epoch": 0.031, "warmup_step": 1.5,
-                 "learned": 29.2, "mixed_cold": 30.3, "fp64_cold": 45.9, "e2e": 29.4, "cpu_sample": 12.0}
+LEARNED_LEG_S = {"start": 20.0, "label_per_instance": 0.0156, "epoch": 0.015, "warmup_step": 1.5,
+                 "learned": 29.2, "mixed_cold": 30.3, "fp64_cold": 45.9, "e2e": 29.4, "cpu_sample": 12.0,
+                 "single_lp": 0.6}
 
 
 def metric_for(args):
@@ -94,6 +95,9 @@ def parse():
     ap.add_argument("--compare-steps", type=int, default=1,
                     help="refinery_learned: steps of each comparison leg (cold mixed, cold FP64)")
     ap.add_argument("--no-fp64", action="store_true", help="skip the plain FP64 comparison leg")
+    ap.add_argument("--single-sample", type=int, default=8,
+                    help="refinery_learned: held-out instances solved one LP per solve by the single-LP FP64 "
+                         "engine (the GPU without the batched engine); 0 skips that comparison")
     ap.add_argument("--time-limit", type=float, default=None,
                     help="single-LP workloads: seconds per solve before it stops as INTERRUPTED "
                          "(default 1200 for ill_conditioned, else none)")
@@ -574,7 +578,8 @@ def learned_cfg(args, fam, world):
             "l2": "per-instance vectors of 2000 instances (~300 MB) exceed L2; the shared matrix is L2-resident",
             "warmup": "warm-up steps run the same solves capped at 2048 iterations (autotuning, graphs, allocations)",
             "steps": {"learned (value)": args.steps, "mixed_cold": args.compare_steps, "fp64_cold": args.compare_steps,
-                      "e2e": args.e2e_steps}}
+                      "e2e": args.e2e_steps, "fp64_single_lp (instances)": args.single_sample},
+            "mlp_training": "batch 1024, Adam lr 2e-3 -> 2e-5 cosine"}
 
 
 def timed_leg(ctx, torch, world, steps, fn):
@@ -603,7 +608,7 @@ def planned_wall_s(args):
             + args.warmup * t["warmup_step"]
             + scale * (args.steps * t["learned"] + args.compare_steps * (t["mixed_cold"] + t["fp64_cold"])
                        + args.e2e_steps * t["e2e"])
-            + t["cpu_sample"])
+            + args.single_sample * t["single_lp"] + t["cpu_sample"])
 
 
 def run_learned_workload(args):
@@ -694,6 +699,31 @@ def run_learned_workload(args):
                "d2h_bytes_per_step": d2h, "steps": args.e2e_steps, "ms_per_step": e2e_ms / args.e2e_steps,
                "solved": int(esolved),
                "note": "batch upload (host CSR checks, renumbering, device transpose, scaling) + learned solve + x, y"}
+    # plain FP64 cold-start PDHG one LP per solve -- the single-LP engine on the same GPU, the
+    # held-out instances one after another -- on the first --single-sample instances: what the
+    # GPU gives without the batched engine (each solve timed with CUDA events on the stream)
+    single = None
+    if args.single_sample > 0:
+        cnt = min(args.single_sample, args.heldout)
+        tot_ms, ok1, its1 = 0.0, 0, []
+        stream = torch.cuda.current_stream()
+        for i in range(cnt):
+            ctx.upload(b2p.lpgen.StdLP(s0.m, s0.n, s0.rowptr, s0.colidx, s0.vals, B[i], Cc[i], LB[i], UB[i], EQ[i]))
+            if i == 0:  # autotune the single-LP kernels for this shape outside the timing
+                ctx.solve(engine="halpern", precision="fp64", max_iterations=2048, **judge)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record(stream)
+            r1, _, _ = ctx.solve(engine="halpern", precision="fp64", max_iterations=cap, **judge)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            tot_ms += e0.elapsed_time(e1)
+            ok1 += int(r1["status"] == "OPTIMAL")
+            its1.append(r1["iterations"])
+        lps = sum_over_ranks(ok1 / (max_over_ranks(tot_ms, world) / 1e3), world)
+        single = {"value": lps, "unit": "LPs/s", "instances": cnt, "solved": ok1, "ms_per_lp": tot_ms / cnt,
+                  "iterations_mean": float(np.mean(its1)),
+                  "engine": "single-LP Halpern engine, FP64, cold start, one LP per solve (same judge)"}
     # roofline of the dominant kernel (the batched chunk kernel of the tuned shape):
     # algorithmic bytes of every instance-iteration of the value leg over its kernel time --
     # the SELL matrix (12 B per nonzero, both orientations) once per CTA-iteration, so once
@@ -739,16 +769,19 @@ def run_learned_workload(args):
                                    if "fp64_cold" in res else HALPERN_ITERS["refinery_learned"])
     if rank == 0:
         ratio = (res["learned"]["value"] / res["fp64_cold"]["value"]) if "fp64_cold" in res else None
+        ratio1 = (res["learned"]["value"] / single["value"]) if single and single["value"] > 0 else None
         line = {"metric": METRIC_LEARNED, "value": res["learned"]["value"], "unit": "LPs/s", "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": res["learned"]["ms_per_step"],
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
                 "dtype": "f32 (SpMV, vectors) + f64 (scaling, KKT, re-centring); bf16 MLP",
                 "data": "synthetic (seeded refinery planning family, no dataset)",
                 "config": learned_cfg(args, fam, world), "learned_vs_fp64_cold": ratio,
+                "learned_vs_fp64_single_lp": ratio1,
                 "judge": {"eps_rel_kkt": args.eps, "eps_objective": args.eps_objective,
                           "counted": "status OPTIMAL: FP64 relative KKT <= eps on the original instance and the "
                                      "FP64 objective-error bound <= eps_objective, both on the device"},
                 "learned": res["learned"], "mixed_cold": res.get("mixed_cold"), "fp64_cold": res.get("fp64_cold"),
+                "fp64_single_lp": single,
                 "training": fit, "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "gpu_launches": launches,
                 "clocks": clocks, "wall_s": time.perf_counter() - t_wall0, "planned_wall_s": plan}
         print(json.dumps(line), flush=True)

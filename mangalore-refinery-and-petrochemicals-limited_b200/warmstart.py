@@ -41,8 +41,8 @@ class LearnedWarmStart:
         self.ctx, self.family, self.hidden, self.seed = ctx, family, hidden, seed
         self.stats = {}
 
-    def fit(self, n_train: int = 20000, label_eps: float = 1e-8, epochs: int = 200, batch: int = 256,
-            lr: float = 1e-3, param_seed: int = 1, max_iterations: int = 1_000_000):
+    def fit(self, n_train: int = 20000, label_eps: float = 1e-8, epochs: int = 200, batch: int = 1024,
+            lr: float = 2e-3, param_seed: int = 1, max_iterations: int = 1_000_000):
         ctx, fam = self.ctx, self.family
         P = fam.sample_params(n_train, param_seed)
         t0 = time.perf_counter()
