@@ -92,6 +92,10 @@ def parse():
     ap.add_argument("--eps-objective", type=float, default=1e-6,
                     help="an answer also needs its objective within this relative distance of the optimum (FP64 "
                          "bound on the device); 0 = relative KKT alone")
+    ap.add_argument("--check-every", type=int, default=128,
+                    help="refinery_learned: iterations between restart checks in every leg (the checks cost "
+                         "half as much at 128 as at the library default 64, and the planning family needs "
+                         "slightly fewer iterations)")
     ap.add_argument("--compare-steps", type=int, default=1,
                     help="refinery_learned: steps of each comparison leg (cold mixed, cold FP64)")
     ap.add_argument("--no-fp64", action="store_true", help="skip the plain FP64 comparison leg")
@@ -138,7 +142,7 @@ def profile_learned(args):
         ws.fit(n_train=1024, label_eps=1e-6, epochs=20, max_iterations=100000)
         b2p.warmstart.upload_family(ctx, fam, P)
         F = P.astype(np.float32)
-        judge = dict(eps=args.eps, eps_objective=args.eps_objective)
+        judge = dict(eps=args.eps, eps_objective=args.eps_objective, check_every=args.check_every)
         legs = {
             "learned": lambda it: ctx.batch_solve_learned(F, precision="fp32", max_iterations=it, outputs=False,
                                                           **judge),
@@ -579,7 +583,7 @@ def learned_cfg(args, fam, world):
             "warmup": "warm-up steps run the same solves capped at 2048 iterations (autotuning, graphs, allocations)",
             "steps": {"learned (value)": args.steps, "mixed_cold": args.compare_steps, "fp64_cold": args.compare_steps,
                       "e2e": args.e2e_steps, "fp64_single_lp (instances)": args.single_sample},
-            "mlp_training": "batch 1024, Adam lr 2e-3 -> 2e-5 cosine"}
+            "mlp_training": "batch 1024, Adam lr 2e-3 -> 2e-5 cosine", "check_every": args.check_every}
 
 
 def timed_leg(ctx, torch, world, steps, fn):
@@ -629,7 +633,7 @@ def run_learned_workload(args):
     F = P.astype(np.float32)
     # every leg stops on the same judge: relative KKT <= eps and the answer's objective
     # within eps_objective of the optimum (FP64 bound evaluated on the device)
-    judge = dict(eps=args.eps, eps_objective=args.eps_objective)
+    judge = dict(eps=args.eps, eps_objective=args.eps_objective, check_every=args.check_every)
     cap = 400000
     legs = {
         "learned": lambda it: ctx.batch_solve_learned(F, fallback=True, precision="fp32", max_iterations=it,
