@@ -142,12 +142,12 @@ def profile_learned(args):
         ws.fit(n_train=1024, label_eps=1e-6, epochs=20, max_iterations=100000)
         b2p.warmstart.upload_family(ctx, fam, P)
         F = P.astype(np.float32)
-        judge = dict(eps=args.eps, eps_objective=args.eps_objective, check_every=args.check_every)
+        stop = dict(eps=args.eps, eps_objective=args.eps_objective, check_every=args.check_every)
         legs = {
             "learned": lambda it: ctx.batch_solve_learned(F, precision="fp32", max_iterations=it, outputs=False,
-                                                          **judge),
-            "mixed_cold": lambda it: ctx.batch_solve(precision="fp32", max_iterations=it, outputs=False, **judge),
-            "fp64_cold": lambda it: ctx.batch_solve(precision="fp64", max_iterations=it, outputs=False, **judge),
+                                                          **stop),
+            "mixed_cold": lambda it: ctx.batch_solve(precision="fp32", max_iterations=it, outputs=False, **stop),
+            "fp64_cold": lambda it: ctx.batch_solve(precision="fp64", max_iterations=it, outputs=False, **stop),
         }
         for fn in legs.values():
             fn(2048)
@@ -456,7 +456,7 @@ def upload_batch(ctx, stds, shared):
 
 
 def run_batch_workload(args):
-    """configs[2] (uneven_batch: 4096 LPs of uneven size, each its own matrix) or the
+    """The uneven batch (4096 LPs of uneven size, each its own matrix) or the
     random-structure refinery family (one shared matrix), cold start: mixed precision
     timed for --steps, plain FP64 for --compare-steps, end to end for --e2e-steps; one
     replica per GPU on its own seed (weak scaling)."""
@@ -468,11 +468,11 @@ def run_batch_workload(args):
     ctx = b2p.Context(local)
     ctx.set_stream(torch.cuda.current_stream().cuda_stream)
     upload_batch(ctx, stds, shared)
-    judge = dict(eps=args.eps, eps_objective=args.eps_objective)
+    stop = dict(eps=args.eps, eps_objective=args.eps_objective)
     cap = 400000
     for _ in range(args.warmup):
         for prec in ("fp32", "fp64"):
-            ctx.batch_solve(precision=prec, max_iterations=2048, outputs=False, **judge)
+            ctx.batch_solve(precision=prec, max_iterations=2048, outputs=False, **stop)
     uuid = None
     try:
         uuid = "GPU-" + str(torch.cuda.get_device_properties(local).uuid)
@@ -487,7 +487,7 @@ def run_batch_workload(args):
             sampler.start()
         ms, (summ, per, _, _) = timed_leg(ctx, torch, world, k,
                                           lambda: ctx.batch_solve(precision=prec, max_iterations=cap, outputs=False,
-                                                                  **judge))
+                                                                  **stop))
         if sampler:
             clocks = sampler.stop()
         solved = sum_over_ranks(float((per["status"] == 0).sum()), world)
@@ -515,7 +515,7 @@ def run_batch_workload(args):
     def e2e_step():
         ctx.batch_upload(mats, inst, pin["b"].numpy(), pin["c"].numpy(), pin["lb"].numpy(), pin["ub"].numpy(),
                          pin["is_eq"].numpy())
-        return ctx.batch_solve(precision="fp32", max_iterations=cap, **judge)
+        return ctx.batch_solve(precision="fp32", max_iterations=cap, **stop)
 
     e2e = {"value": None, "skipped": "--e2e-steps 0", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h}
     if args.e2e_steps > 0:
@@ -631,15 +631,15 @@ def run_learned_workload(args):
     fit = ws.fit(n_train=args.train_count, label_eps=args.label_eps, epochs=args.epochs)
     s0 = b2p.warmstart.upload_family(ctx, fam, P)
     F = P.astype(np.float32)
-    # every leg stops on the same judge: relative KKT <= eps and the answer's objective
+    # every leg stops on the same rule: relative KKT <= eps and the answer's objective
     # within eps_objective of the optimum (FP64 bound evaluated on the device)
-    judge = dict(eps=args.eps, eps_objective=args.eps_objective, check_every=args.check_every)
+    stop = dict(eps=args.eps, eps_objective=args.eps_objective, check_every=args.check_every)
     cap = 400000
     legs = {
         "learned": lambda it: ctx.batch_solve_learned(F, fallback=True, precision="fp32", max_iterations=it,
-                                                      outputs=False, **judge),
-        "mixed_cold": lambda it: ctx.batch_solve(precision="fp32", max_iterations=it, outputs=False, **judge),
-        "fp64_cold": lambda it: ctx.batch_solve(precision="fp64", max_iterations=it, outputs=False, **judge),
+                                                      outputs=False, **stop),
+        "mixed_cold": lambda it: ctx.batch_solve(precision="fp32", max_iterations=it, outputs=False, **stop),
+        "fp64_cold": lambda it: ctx.batch_solve(precision="fp64", max_iterations=it, outputs=False, **stop),
     }
     for _ in range(args.warmup):
         for fn in legs.values():
@@ -693,7 +693,7 @@ def run_learned_workload(args):
     def e2e_step():
         ctx.batch_upload([(s0.m, s0.n, s0.rowptr, s0.colidx, s0.vals)], np.zeros(args.heldout, np.int32),
                          pin["b"].numpy(), pin["c"].numpy(), pin["lb"].numpy(), pin["ub"].numpy(), pin["is_eq"].numpy())
-        return ctx.batch_solve_learned(pin["f"].numpy(), fallback=True, precision="fp32", max_iterations=cap, **judge)
+        return ctx.batch_solve_learned(pin["f"].numpy(), fallback=True, precision="fp32", max_iterations=cap, **stop)
 
     e2e = {"value": None, "skipped": "--e2e-steps 0", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h}
     if args.e2e_steps > 0:
@@ -714,11 +714,11 @@ def run_learned_workload(args):
         for i in range(cnt):
             ctx.upload(b2p.lpgen.StdLP(s0.m, s0.n, s0.rowptr, s0.colidx, s0.vals, B[i], Cc[i], LB[i], UB[i], EQ[i]))
             if i == 0:  # autotune the single-LP kernels for this shape outside the timing
-                ctx.solve(engine="halpern", precision="fp64", max_iterations=2048, **judge)
+                ctx.solve(engine="halpern", precision="fp64", max_iterations=2048, **stop)
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             torch.cuda.synchronize()
             e0.record(stream)
-            r1, _, _ = ctx.solve(engine="halpern", precision="fp64", max_iterations=cap, **judge)
+            r1, _, _ = ctx.solve(engine="halpern", precision="fp64", max_iterations=cap, **stop)
             e1.record(stream)
             torch.cuda.synchronize()
             tot_ms += e0.elapsed_time(e1)
@@ -727,7 +727,7 @@ def run_learned_workload(args):
         lps = sum_over_ranks(ok1 / (max_over_ranks(tot_ms, world) / 1e3), world)
         single = {"value": lps, "unit": "LPs/s", "instances": cnt, "solved": ok1, "ms_per_lp": tot_ms / cnt,
                   "iterations_mean": float(np.mean(its1)),
-                  "engine": "single-LP Halpern engine, FP64, cold start, one LP per solve (same judge)"}
+                  "engine": "single-LP Halpern engine, FP64, cold start, one LP per solve (same stop rule)"}
     # roofline of the dominant kernel (the batched chunk kernel of the tuned shape):
     # algorithmic bytes of every instance-iteration of the value leg over its kernel time --
     # the SELL matrix (12 B per nonzero, both orientations) once per CTA-iteration, so once
@@ -781,7 +781,7 @@ def run_learned_workload(args):
                 "data": "synthetic (seeded refinery planning family, no dataset)",
                 "config": learned_cfg(args, fam, world), "learned_vs_fp64_cold": ratio,
                 "learned_vs_fp64_single_lp": ratio1,
-                "judge": {"eps_rel_kkt": args.eps, "eps_objective": args.eps_objective,
+                "stop_rule": {"eps_rel_kkt": args.eps, "eps_objective": args.eps_objective,
                           "counted": "status OPTIMAL: FP64 relative KKT <= eps on the original instance and the "
                                      "FP64 objective-error bound <= eps_objective, both on the device"},
                 "learned": res["learned"], "mixed_cold": res.get("mixed_cold"), "fp64_cold": res.get("fp64_cold"),

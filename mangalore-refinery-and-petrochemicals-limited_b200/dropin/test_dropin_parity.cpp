@@ -6,7 +6,7 @@
 // B200 reference engine to return what CPUFirstOrderSolver returns: the same
 // status, the same iteration count, and bit-identical primal and dual vectors
 // and objective.  They also exercise the Halpern engine through the drop-in and
-// the router, judged by the reference's SolutionVerifier.
+// the router, checked by the reference's SolutionVerifier.
 #include "test_harness.hpp"
 
 #include <bharatopt/benchmark_framework.hpp>
@@ -118,7 +118,7 @@ TEST_CASE(DropIn_04_IterationLimitOnGpu) {
 
 TEST_CASE(DropIn_05_HalpernEngineVerified) {
     // the Halpern engine to 1e-9 relative KKT through the drop-in; the reference's own
-    // dual simplex gives the objective it must match, the verifier judges the point
+    // dual simplex gives the objective it must match, the verifier checks the point
     LPModel model = generated("square", 120, 60, 99, 0.1);
     b2p_params p;
     b2p_params_default(&p);
@@ -409,7 +409,7 @@ TEST_CASE(DropIn_12_DirectSetupMatchesAndSkipsHostPresolve) {
     vo.feasibility_tolerance = 1e-5;
     EXPECT_TRUE(ver.verify(small, b.primal_solution, vo).verified);
     // ranged rows: the direct setup keeps both ends (the reference front end keeps only the
-    // lower end), judged by the reference's verifier, which reads both
+    // lower end), checked by the reference's verifier, which reads both
     LPModel rng = random_model(300, 900, 3, 13, true);
     FirstOrderSolverResult e = FirstOrderLPSolver(o).solve(rng);
     EXPECT_EQ(e.status, FirstOrderSolverStatus::OPTIMAL);

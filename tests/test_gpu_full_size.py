@@ -1,4 +1,4 @@
-"""The benchmark's full-size workloads on the GPU, judged by the oracle's FP64 KKT.
+"""The benchmark's full-size workloads on the GPU, checked with the oracle's FP64 KKT.
 
 * block-angular blending LP (m = 204,000, n = 1,000,000, 8.0M nonzeros): single-LP
   engine, mixed precision and FP64, to 1e-6 relative KKT;

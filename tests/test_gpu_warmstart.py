@@ -1,7 +1,7 @@
 """Learned warm start on the GPU: training set from the engine's own answers,
 tensor-core training, MLP-predicted warm starts with the cold-start fallback.
 
-Every warm-started answer checked here is judged by the oracle's FP64 KKT; the
+Every warm-started answer checked here is checked by the oracle's FP64 KKT; the
 gain test compares the trained network against the same engine without it."""
 from __future__ import annotations
 
