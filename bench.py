@@ -41,7 +41,7 @@ sys.path.insert(0, str(ROOT))
 # extrapolates the reference CPU solver's per-iteration cost over this many
 # iterations -- generous to the CPU: the reference's own vanilla PDHG needs far
 # more iterations and never reaches 1e-6 on these LPs.
-HALPERN_ITERS = {"block_angular": 6784, "random_sparse": 5056, "refinery_learned": 111851, "uneven_batch": 6379,
+HALPERN_ITERS = {"block_angular": 6784, "random_sparse": 5056, "refinery_learned": 110744, "uneven_batch": 6379,
                  # mixed engine to 1e-8 (the FP64 leg of this workload was not run)
                  "ill_conditioned": 1230784}
 
