@@ -23,7 +23,10 @@
 //     between external and internal order on the device.
 // Execution
 //   * one CTA owns one instance at a time (persistent grid, work queue sorted by
-//     nnz descending = longest-first).  The gathered operands of both SpMVs --
+//     nnz descending = longest-first) -- or, in the paired form for batches whose
+//     instances share one matrix, two instances iterated in lockstep so that each
+//     SELL load feeds both.  When a CTA takes an instance it copies its matrix's
+//     slice pointers into a shared-memory table.  The gathered operands of both SpMVs --
 //     y (also the dual iterate) for A^T y and xh for A xh -- live in shared
 //     memory; x and the packed records stay in global memory, touched only by
 //     their owning thread.  A PDHG iteration is: primal phase (one thread per
@@ -41,13 +44,15 @@
 //     l - xbar, u - xbar, dual bound -ybar, rebuilt from the FP64 matrix, so
 //     the FP32 iterates only carry the correction (iterative refinement).
 //   * per instance: own step size (from its matrix), primal weight, Halpern
-//     counter, restart state, FP64 KKT every K iterations (block reductions in a
+//     counter, restart state, FP64 KKT every K iterations (over FP64 SELL copies
+//     with the checked vectors staged in shared memory; block reductions in a
 //     fixed order: deterministic), own termination.
 //   * a launch runs every active instance for up to `chunk` iterations; a
 //     compaction kernel drops finished instances; [chunk, compact] x 2 is
 //     captured as a CUDA graph and replayed until no instance is active.
-//   * block size comes from an autotuner that times the candidates on a sample
-//     of the batch (cached on disk).
+//   * CTA size, SELL entry order (one entry or a pair per lane load), form
+//     (single or paired) and chunk length come from an autotuner that times the
+//     candidates on a sample of the batch (cached on disk).
 #include <cub/cub.cuh>
 
 #include <algorithm>
