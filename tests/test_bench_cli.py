@@ -26,6 +26,9 @@ def test_workload_defaults(monkeypatch):
     a = _parse(monkeypatch)
     assert a.workload == "refinery_learned" and a.eps == 1e-6 and a.steps == 1 and a.gpus == 1
     assert a.warmup >= 3
+    # every leg of the learned workload stops on relative KKT and the objective criterion,
+    # checking every 256 iterations, and the one-LP-per-solve FP64 comparison runs 8 instances
+    assert a.eps_objective == 1e-6 and a.check_every == 256 and a.single_sample == 8
     a = _parse(monkeypatch, "--workload", "block_angular")
     assert a.eps == 1e-6 and a.steps == 5 and a.time_limit == 0.0 and a.e2e_steps == 5
     a = _parse(monkeypatch, "--workload", "ill_conditioned")
